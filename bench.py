@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Throughput of the projection-method time step on B200 (Mcell-steps/s).
+
+Workload: the 128^3 lid-driven cavity (Re=1000, dt=5e-4, zero initial
+fields), one step = one pass of the loop body (predictor, red-black SOR
+pressure solve to zeta = 1e-4, projection + direct forcing + force integral,
+boundary conditions).  The timed region runs exactly --steps steps starting
+from the initial state (after --warmup untimed steps and a reset); by
+default 500 steps, i.e. the whole case.  The mixed-precision step is the
+headline; the plain FP64 step runs on the same steps for the speed-up and
+the relative L2 error.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--gpus N > 1 runs one independent replica per GPU (the case does not shard
+across GPUs); value = total cells * steps / max-over-ranks device time.
+--impl reference times the CPU restatement of the reference's own algorithm
+(lexicographic SOR with the reference's OpenMP loop schedule) on the host
+cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-steps/s mixed-prec vs FP64 plain at ≤1e-6 rel L2; adjoint/forward cost"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--n", type=int, default=128, help="cavity cells per side")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ ranks
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def aggregate(values, op):
+    """Reduces one float per rank (max or sum) over torch.distributed when
+    it is initialised; identity on a single process."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(values)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(values)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        dist.barrier()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.1)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx = float(f[2].split()[0])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def cavity_case(n, precision, device):
+    from ntustcfdlab_b200 import cases
+    c = cases.cavity(n, 1000.0, 5e-4, 500, precision=precision)
+    c.params.device = device
+    return c
+
+
+def reset(s):
+    z = np.zeros(s.halo_shape, order="F")
+    s.set_state(z, z, z, z)
+    s.boundary_conditions()
+
+
+def timed_run(case, K, W, sampler_index=None):
+    """W warm-up steps, reset to the initial state, then K device-timed steps."""
+    from ntustcfdlab_b200.solver import Solver
+    import torch
+    s = Solver(case.params, case.grid)
+    s.boundary_conditions()
+    if W > 0:
+        s.step(W)
+    reset(s)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = None
+    if sampler_index is not None:
+        with ClockSampler(sampler_index) as cs:
+            info, rc = s.step(K)
+        clocks = cs.summary()
+    else:
+        info, rc = s.step(K)
+    torch.cuda.synchronize()
+    barrier()
+    ms = s.last_step_ms()
+    return s, info, rc, ms, clocks
+
+
+def e2e_run(case, K, isto=100):
+    """The same K steps through the C-ABI with host buffers: upload the
+    initial state from pinned host memory, one ntcfd_step(ctx, 1, &info) per
+    step (info back to the host every step, as the reference driver prints
+    it), centred output fields to the host every `isto` steps
+    (filereachtime cadence, main.f90:317-324) and the final state."""
+    import torch
+    from ntustcfdlab_b200.solver import Solver
+    s = Solver(case.params, case.grid)
+    s.boundary_conditions()
+    s.step(2)                       # graph instantiation outside the timed region
+    shape = s.halo_shape
+    n_halo = int(np.prod(shape))
+    n_in = int(np.prod(s.inner_shape))
+    pin = lambda n: torch.zeros(n, dtype=torch.float64, pin_memory=True).numpy()
+    state = [pin(n_halo).reshape(shape, order="F") for _ in range(4)]
+    outs = [pin(n_in).reshape(s.inner_shape, order="F") for _ in range(4)]
+    back = [pin(n_halo).reshape(shape, order="F") for _ in range(4)]
+    from ntustcfdlab_b200.abi import dptr
+    lib, h = s.lib, s.h
+    from ntustcfdlab_b200.abi import NtcfdStepInfo
+    info = NtcfdStepInfo()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lib.ntcfd_set_state(h, *[dptr(a) for a in state])
+    lib.ntcfd_apply_bc(h)
+    h2d = 4 * n_halo * 8
+    d2h = 0
+    for k in range(1, K + 1):
+        rc = lib.ntcfd_step(h, 1, info)
+        if rc < 0:
+            raise RuntimeError(s._err())
+        d2h += 40  # the step record (StepRec) crosses back every step
+        if k % isto == 0:
+            lib.ntcfd_get_output(h, *[dptr(a) for a in outs])
+            d2h += 4 * n_in * 8
+    lib.ntcfd_get_state(h, *[dptr(a) for a in back])
+    d2h += 4 * n_halo * 8
+    t1 = time.perf_counter()
+    s.close()
+    return (t1 - t0), h2d, d2h
+
+
+def cpu_baseline_from(s_gpu, case, seconds):
+    """Oracle (the CPU restatement of the reference's algorithm, lexicographic
+    SOR with the reference's OpenMP schedule, all host threads) on a bounded
+    sample: consecutive steps from the device state at the end of the timed
+    run, until `seconds` of CPU time have passed."""
+    from oracle import cpu_oracle
+    from ntustcfdlab_b200.abi import SOR_LEX, params_copy
+    threads = os.cpu_count() or 1
+    o = cpu_oracle.Oracle(params_copy(case.params, sor_order=SOR_LEX), case.grid, threads=threads)
+    o.initial_conditions()
+    for k, a in zip("uvwp", s_gpu.get_state()):
+        o.set(k, a)
+    o.boundary_conditions()
+    t0 = time.perf_counter()
+    steps = sweeps = 0
+    while True:
+        inf = o.step(1)[0]
+        steps += 1
+        sweeps += inf.sor_iters
+        el = time.perf_counter() - t0
+        if el >= seconds or steps >= 50:
+            break
+    return case.cells * steps / el / 1e6, threads, steps, sweeps, el
+
+
+def roofline(s, case, reps=20):
+    """Dominant kernel: the half-sweep of the SOR solve.  Algorithmic bytes
+    per half-sweep launch: 3 S per cell per full red+black sweep (read e and
+    d, write e; S = 4 B in mixed, 8 B in FP64), i.e. 1.5 S per cell per launch."""
+    kt = s.time_kernels(reps)
+    S = 4 if case.params.precision == 1 else 8
+    alg = 1.5 * S * case.cells
+    ms = kt["sweep_ms"]
+    ach = alg / (ms * 1e-3) / 1e9
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    if os.path.exists(tp):
+        try:
+            tr = json.load(open(tp))
+            if tr.get("cells") == case.cells and tr.get("bytes_per_element") == S:
+                traffic = tr.get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    return {"kernel": "k_sweep (one colour of a red-black SOR sweep)", "bound": "hbm",
+            "achieved": round(ach, 1), "peak": peak,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
+            "unit": "GB/s", "frac": round(ach / peak, 3), "traffic": traffic,
+            "algorithmic_bytes_per_launch": alg, "avg_launch_ms": ms,
+            "kernel_ms": {k: round(v, 5) for k, v in kt.items()}}
+
+
+def rel_l2(a, b):
+    a = a[2:-2, 2:-2, 2:-2]
+    b = b[2:-2, 2:-2, 2:-2]
+    nb = float(np.linalg.norm(b))
+    return float(np.linalg.norm(a - b)) / nb if nb > 0 else float(np.linalg.norm(a - b))
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from ntustcfdlab_b200.abi import FP64, MIXED
+    K, W = args.steps, max(args.warmup, 0)
+    mixed = cavity_case(args.n, MIXED, local)
+    s, info, rc, ms, clocks = timed_run(mixed, K, W, sampler_index=local)
+    ms_max = aggregate(ms, "max")
+    cells_total = mixed.cells * world
+    value = cells_total * K / (ms_max * 1e-3) / 1e6
+    sweeps = [i.sor_iters for i in info]
+    launches = int(sum(i.launches for i in info))
+    extra = {}
+    if not args.no_fp64:
+        f64 = cavity_case(args.n, FP64, local)
+        s64, info64, _, ms64, _ = timed_run(f64, K, W)
+        ms64_max = aggregate(ms64, "max")
+        v64 = cells_total * K / (ms64_max * 1e-3) / 1e6
+        st32, st64 = s.get_state(), s64.get_state()
+        extra["fp64"] = {"value": round(v64, 2), "ms_per_step": ms64_max / K,
+                         "sweeps_total": int(sum(i.sor_iters for i in info64))}
+        extra["mixed_over_fp64"] = round(value / v64, 3)
+        extra["rel_l2_mixed_vs_fp64"] = {k: rel_l2(a, b) for k, a, b in zip("uvwp", st32, st64)}
+        s64.close()
+    e2e = None
+    if not args.no_e2e:
+        t, h2d, d2h = e2e_run(mixed, K)
+        t_max = aggregate(t, "max")
+        e2e = {"value": round(cells_total * K / t_max / 1e6, 2), "unit": UNIT,
+               "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+               "timing": "host wall clock around the synchronous C-ABI calls"}
+    rl = roofline(s, mixed) if rank == 0 else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, thr, nst, nsw, el = cpu_baseline_from(s, mixed, args.cpu_seconds)
+        cpu = {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": (f"{nst} consecutive steps ({nsw} SOR sweeps, {el:.1f} s) of the same "
+                          f"{args.n}^3 case from the device state after step {K}; lexicographic "
+                          f"SOR with the reference's OpenMP schedule, {thr} threads")}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (lid-driven cavity from rest, no dataset)",
+            "config": {"workload": f"lid-driven cavity {args.n}^3, Re=1000, dt=5e-4, zeta=1e-4, "
+                                   f"mixed precision (FP32 red-black SOR + FP64 defect correction)",
+                       "grid": [args.n] * 3, "case_steps": 500,
+                       "l2": "inputs larger than L2: state is 9 FP64 arrays of "
+                             f"{(args.n + 4) ** 3 * 8 / 1e6:.0f} MB, no flush",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "sor_sweeps_total": int(sum(sweeps)), "sor_sweeps_per_step": float(np.mean(sweeps)),
+            "all_converged": bool(all(i.converged for i in info)),
+            "gpu_launches": launches * world,
+            "adjoint_over_forward": None,
+            "roofline": rl, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        barrier()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import cpu_oracle
+    from ntustcfdlab_b200.abi import SOR_LEX, params_copy
+    from ntustcfdlab_b200 import cases
+    from ntustcfdlab_b200.abi import MIXED
+    c = cases.cavity(args.n, 1000.0, 5e-4, 500, precision=MIXED)
+    threads = os.cpu_count() or 1
+    o = cpu_oracle.Oracle(params_copy(c.params, sor_order=SOR_LEX), c.grid, threads=threads)
+    o.initial_conditions()
+    o.boundary_conditions()
+    if args.warmup > 0:
+        o.step(args.warmup)
+    budget = 150.0
+    t0 = time.perf_counter()
+    done = sweeps = 0
+    for _ in range(args.steps):
+        inf = o.step(1)[0]
+        done += 1
+        sweeps += inf.sor_iters
+        if time.perf_counter() - t0 > budget:
+            break
+    el = time.perf_counter() - t0
+    value = c.cells * done / el / 1e6
+    sample = (f"steps {args.warmup + 1}-{args.warmup + done} of the {args.n}^3 cavity from rest "
+              f"({sweeps} SOR sweeps, {el:.1f} s; at most {budget:.0f} s of steps)")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": 0, "steps": done, "warmup": args.warmup, "ms_per_step": el * 1e3 / done,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (lid-driven cavity from rest, no dataset)",
+            "config": {"workload": f"lid-driven cavity {args.n}^3, Re=1000, dt=5e-4, zeta=1e-4",
+                       "grid": [args.n] * 3, "parallelism": f"{threads} OpenMP threads"},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the Fortran/MPI reference cannot be compiled here (no Fortran compiler, no "
+                    "MPI); this arm runs the C++ restatement of its algorithm with the reference's "
+                    "lexicographic SOR and OpenMP loop schedule"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

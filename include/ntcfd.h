@@ -1,0 +1,172 @@
+/*
+ * ntcfd.h -- C-ABI of the B200 projection-method time step.
+ *
+ * This is the drop-in boundary for NTUSTCFD's time-step loop body
+ * (main.f90:209-259): Smagorinsky viscosity, QUICK predictor, SOR pressure
+ * Poisson solve, projection, direct-forcing immersed boundary, force
+ * integral, velocity update and boundary conditions.  The reference calls
+ * argument-less Fortran subroutines that work on MODULE variables
+ * (variables_module.f90); here the same state lives in device memory owned
+ * by an opaque context, and the Fortran driver reaches it through
+ * ISO_C_BINDING (see fortran/ntcfd_iface.f90).
+ *
+ * Conventions shared by every entry point:
+ *  - Halo arrays are Fortran order (i fastest), index range -1..n+2 in each
+ *    direction, i.e. (nx+4)*(ny+4)*(nz+4) doubles, exactly the layout of
+ *    `real*8, dimension(-1:nx+2,-1:ny+2,-1:nz+2)` in variables_module.f90:215-223.
+ *  - Interior arrays (pre, uc, vc, wc) are (nx,ny,nz), Fortran order
+ *    (variables_module.f90:225).
+ *  - 1-D metrics iDx/Dxs/... have n+4 entries, index -1..n+2
+ *    (variables_module.f90:306-316); node coordinates X/Y/Z have n+5
+ *    entries, index -1..n+3 (variables_module.f90:292-296).
+ *  - Every pointer argument is HOST memory; calls are synchronous at return.
+ *  - Every call returns 0 on success, a negative NTCFD_E* code on error
+ *    (ntcfd_last_error() gives the message), or the positive warning
+ *    NTCFD_NOT_CONVERGED when an SOR solve stopped at itmax (the reference
+ *    continues silently in that case, GS.f90:11).
+ *  - A context is used by one host thread at a time and owns one CUDA stream.
+ */
+#ifndef NTCFD_H
+#define NTCFD_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NTCFD_OK              0
+#define NTCFD_NOT_CONVERGED   1   /* warning: at least one SOR solve hit itmax */
+#define NTCFD_EINVAL        (-1)  /* bad parameter or argument */
+#define NTCFD_ECUDA         (-2)  /* CUDA runtime error */
+#define NTCFD_ENOMEM        (-3)  /* device allocation failed */
+#define NTCFD_ENONFINITE    (-4)  /* NaN/Inf detected in the SOR residual */
+#define NTCFD_ESTATE        (-5)  /* call out of order (e.g. no metrics yet) */
+#define NTCFD_ETIMEOUT      (-6)  /* a bounded device wait gave up */
+
+/* Boundary-condition kinds: the strings 'no-slip', 'Neumann', 'Dirichlet'
+ * of variables_module.f90:110-132, plus PERIODIC (no reference counterpart). */
+enum { NTCFD_BC_NOSLIP = 0, NTCFD_BC_NEUMANN = 1, NTCFD_BC_DIRICHLET = 2,
+       NTCFD_BC_PERIODIC = 3 };
+/* Walls, in the order boundary_conditions.f90 applies them (13-301). */
+enum { NTCFD_WEST = 0, NTCFD_EAST = 1, NTCFD_SOUTH = 2, NTCFD_NORTH = 3,
+       NTCFD_BACK = 4, NTCFD_FRONT = 5 };
+enum { NTCFD_FP64 = 0, NTCFD_MIXED = 1 };
+enum { NTCFD_QUICK_CENTRE = 0 };                       /* discretisation_QUICK_centre.f90 */
+enum { NTCFD_SMAG_REF_ALIASED = 0, NTCFD_SMAG_STAGGERED = 1 };
+enum { NTCFD_SOR_REDBLACK = 0, NTCFD_SOR_LEX = 1 };    /* LEX: oracle only */
+
+typedef struct ntcfd_params {
+    int nx, ny, nz;          /* interior cells (variables_module.f90:13-17) */
+    double Re;               /* nu = 1/Re (reading_data.f90:38) */
+    double dt;               /* time step (variables_module.f90:11) */
+    double omega;            /* SOR relaxation (main.f90:44) */
+    double zeta;             /* SOR stop: max|pNew-p| <= zeta (main.f90:46, GS.f90:11) */
+    int itmax;               /* SOR sweep cap (main.f90:48) */
+    int LES;                 /* 1: add Smagorinsky nu_t (main.f90:60) */
+    double Cs;               /* Smagorinsky constant (variables_module.f90:277) */
+    int scheme;              /* NTCFD_QUICK_CENTRE */
+    int precision;           /* NTCFD_FP64 or NTCFD_MIXED */
+    int sor_order;           /* NTCFD_SOR_REDBLACK on the device */
+    int smag_mode;           /* NTCFD_SMAG_REF_ALIASED (reference indexing) or _STAGGERED */
+    int check_every;         /* test the SOR stop rule every c sweeps (1 = every sweep) */
+    int bc[6][3];            /* [wall][u,v,w] kind */
+    double bc_value[6][3];   /* Dirichlet value (the reference hard-codes 1.0) */
+    double u_solid[3];       /* solid velocity in the forcing (variables_module.f90:331-335) */
+    double lx;               /* force-coefficient normalisation (virtualForceIntegrator.f90:80-81) */
+    int mixed_cycle;         /* MIXED: max FP32 sweeps per defect-correction cycle (0 = itmax) */
+    int diag_divergence;     /* 1: report max|div u^{n+1}| in ntcfd_step_info.div_max */
+    int device;              /* CUDA device ordinal that holds the grid */
+    int reserved[5];         /* must be zero */
+} ntcfd_params;
+
+typedef struct ntcfd_step_info {
+    int sor_iters;           /* sweeps this step (GS.f90:96-103 prints the same count) */
+    int converged;           /* 1 if the stop rule fired before itmax */
+    double sor_last_change;  /* max|pNew-p| of the last checked sweep */
+    double cDrag, cLift;     /* virtualForceIntegrator.f90:80-81 */
+    double div_max;          /* max |div u^{n+1}| * V (FP64) when diag_divergence = 1 */
+    int dc_cycles;           /* defect-correction cycles used */
+    int launches;            /* device kernels launched for this step */
+} ntcfd_step_info;
+
+/* Average device time of single kernels of the step, for the roofline. */
+typedef struct ntcfd_kernel_times {
+    float predictor_ms;      /* K2 (with K1 when LES = 1), one launch */
+    float rhs_ms;            /* K3a */
+    float defect_ms;         /* defect pass of a correction cycle */
+    float sweep_ms;          /* one half-sweep (one colour) */
+    float project_ms;        /* K4, measured on a copy of the velocity */
+    float bc_ms;             /* the three K6 launches together */
+    float reserved[2];
+} ntcfd_kernel_times;
+
+typedef struct ntcfd_ctx ntcfd_ctx;
+
+/* Fills p with the reference defaults: 40^3, Re=10, dt=1e-3, omega=1.5,
+ * zeta=1e-4, itmax=3000, LES=0, Cs=0.18, cavity walls with the lid on the
+ * north wall moving in w (variables_module.f90:9-23,110-132,277; main.f90:44-60). */
+void ntcfd_default_params(ntcfd_params* p);
+
+/* Replaces program init: allocation of the MODULE arrays and
+ * initial_conditions() (initial_conditions.f90:9-29, all fields zero). */
+int  ntcfd_create(const ntcfd_params* p, ntcfd_ctx** out);
+void ntcfd_destroy(ntcfd_ctx* ctx);
+const char* ntcfd_last_error(const ntcfd_ctx* ctx);
+
+/* Grid metrics made by gridder_equal/gridder_Unequal (gridder.f90:97-157). */
+int ntcfd_set_metrics(ntcfd_ctx* ctx,
+                      const double* iDx, const double* Dxs,
+                      const double* iDy, const double* Dys,
+                      const double* iDz, const double* Dzs);
+/* Node coordinates X, Y, Z (gridder.f90:34-93); needed by the mask builders. */
+int ntcfd_set_coords(ntcfd_ctx* ctx, const double* X, const double* Y, const double* Z);
+
+/* Volume fraction ETA (variables_module.f90:159), a halo array. */
+int ntcfd_set_mask(ntcfd_ctx* ctx, const double* eta);
+int ntcfd_get_mask(ntcfd_ctx* ctx, double* eta);
+/* RayCasting (airfoil.f90:580-915) on the device: polygon (az[m], ay[m]),
+ * m < npts, is shifted by -0.25, rotated by -aoa_deg, moved to (zc, yc) and
+ * scan-converted into ETA with 50x50 sub-cells on cut cells.  ties_out
+ * (may be NULL) receives the number of exact vertex/grid ties met, which
+ * the reference resolves by moving the grid (airfoil.f90:700-702). */
+int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
+                             double aoa_deg, double zc, double yc, int* ties_out);
+/* DFIB_Cylinder (DFIB.f90:74-145): cylinder along x, centre (zc, yc), radius r,
+ * 50x50 sub-cells within half a cell diagonal of the surface, real*4 arithmetic. */
+int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r);
+
+/* Velocity and pressure halo arrays in and out (exact FP64 checkpoints). */
+int ntcfd_set_state(ntcfd_ctx* ctx, const double* u, const double* v,
+                    const double* w, const double* p);
+int ntcfd_get_state(ntcfd_ctx* ctx, double* u, double* v, double* w, double* p);
+
+/* boundary_conditions() (boundary_conditions.f90:13-374) on the device
+ * state; the driver calls it once after ntcfd_set_state, as main.f90:100 does. */
+int ntcfd_apply_bc(ntcfd_ctx* ctx);
+
+/* Output fields of the last completed step: pre = p after the SOR solve
+ * (GS.f90:86-94) and the centred velocities uc, vc, wc computed from the
+ * projected, forced velocity before the end-of-step boundary conditions
+ * (calcul_new_velocity.f90:171-181).  Each (nx,ny,nz); any may be NULL. */
+int ntcfd_get_output(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc);
+
+/* nsteps passes of the loop body main.f90:209-259 plus `time += dt`.
+ * per_step (nsteps entries) may be NULL. */
+int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* per_step);
+
+/* Simulated time (main.f90:271). */
+double ntcfd_time(const ntcfd_ctx* ctx);
+
+/* Device time of the last ntcfd_step call: CUDA events recorded on the
+ * context's stream before the first and after the last step launch. */
+int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms);
+
+/* Times `reps` standalone launches of each step kernel on the context's
+ * stream with CUDA events and returns the averages.  The velocity, pressure
+ * and ETA of the context are left unchanged. */
+int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NTCFD_H */

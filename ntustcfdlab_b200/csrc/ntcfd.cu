@@ -1,0 +1,876 @@
+// ntcfd.cu -- device context and C-ABI of the B200 projection-method step.
+//
+// One context = one grid resident in device memory + one CUDA stream + one
+// instantiated CUDA graph holding a whole time step (main.f90:209-259).  The
+// SOR loop of gauss_seidel (GS.f90:11) runs on the device as a nested pair
+// of conditional WHILE nodes (defect-correction cycles around red-black
+// sweeps), so a step needs no host round trip; ntcfd_step(n) launches the
+// graph n times and copies back one small record per step.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/ntcfd.h"
+#include "k_mask.cuh"
+#include "k_predictor.cuh"
+#include "k_pressure.cuh"
+#include "k_project.cuh"
+#include "ntcfd_common.cuh"
+
+using namespace ntcfd;
+
+namespace {
+
+constexpr int kProjKc = 8;      // planes per column chunk in K4
+constexpr int kSweepBx = 64;    // threads per row in a half-sweep
+constexpr int kSweepBy = 4;
+
+struct DevTabs {
+    // one allocation per precision; every table has n+5 entries (index -2..n+2)
+    void* buf = nullptr;
+};
+
+}  // namespace
+
+struct ntcfd_ctx {
+    ntcfd_params prm{};
+    std::string err;
+    cudaStream_t stream = nullptr;
+    Geom g{};
+    size_t nat_elems = 0, spl_elems = 0;
+    double *u = nullptr, *v = nullptr, *w = nullptr, *p = nullptr;
+    double *us = nullptr, *vs = nullptr, *ws = nullptr, *b = nullptr;
+    double *eta = nullptr, *nut = nullptr;
+    void *eR = nullptr, *eB = nullptr, *dR = nullptr, *dB = nullptr;
+    double* tabd = nullptr;   // double tables
+    float* tabf = nullptr;    // float tables
+    Tabs<double> tpd{};
+    Tabs<float> tpf{};
+    SorCoef<double> scd{};
+    SorCoef<float> scf{};
+    double *partZ = nullptr, *partY = nullptr, *FXz = nullptr, *FYz = nullptr;
+    double *faceW = nullptr, *faceE = nullptr, *faceS = nullptr, *faceN = nullptr;
+    double *faceB = nullptr, *faceF = nullptr;
+    double* outbuf = nullptr;   // pre, uc, vc, wc
+    double *coordY = nullptr, *coordZ = nullptr;  // node coordinates (pre-offset)
+    double* coordbuf = nullptr;
+    Ctl* ctl = nullptr;
+    StepRec* rec = nullptr;
+    int rec_cap = 0;
+    unsigned long long* slots = nullptr;   // per-sweep max |change| bits
+    unsigned long long* divslot = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.0f;
+    bool metrics_set = false, coords_set = false;
+    double time = 0.0;
+    int nchunk = 0, csweeps = 1, cycle_len = 1;
+    std::vector<void*> allocs;
+};
+
+namespace {
+
+int fail(ntcfd_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? NTCFD_ENOMEM : NTCFD_ECUDA, \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                        \
+    } while (0)
+
+// Every entry point that touches the device selects the context's device
+// first: the caller may have another device current on this thread.
+#define DEV()                                                                         \
+    do {                                                                              \
+        if (!ctx || !ctx->stream) return NTCFD_ESTATE;                                \
+        CK(cudaSetDevice(ctx->prm.device));                                           \
+    } while (0)
+
+template <class T>
+int dalloc(ntcfd_ctx* ctx, T** ptr, size_t n) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, n * sizeof(T) + 256));
+    CK(cudaMemsetAsync(q, 0, n * sizeof(T) + 256, ctx->stream));
+    ctx->allocs.push_back(q);
+    *ptr = reinterpret_cast<T*>(q);
+    return 0;
+}
+
+dim3 grid3(const Geom& g, dim3 b) {
+    return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, (g.nz + b.z - 1) / b.z);
+}
+
+// ---- graph construction helpers
+template <class Tuple, size_t... I>
+void fill_ptrs(Tuple& t, void** p, std::index_sequence<I...>) {
+    ((p[I] = (void*)&std::get<I>(t)), ...);
+}
+
+template <class... KArgs, class... Args>
+cudaError_t add_kernel(cudaGraphNode_t* out, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+                       void (*f)(KArgs...), dim3 grid, dim3 block, Args&&... args) {
+    std::tuple<KArgs...> t(std::forward<Args>(args)...);
+    void* ptrs[sizeof...(KArgs) > 0 ? sizeof...(KArgs) : 1];
+    fill_ptrs(t, ptrs, std::index_sequence_for<KArgs...>{});
+    cudaKernelNodeParams kp{};
+    kp.func = (void*)f;
+    kp.gridDim = grid;
+    kp.blockDim = block;
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = ptrs;
+    kp.extra = nullptr;
+    return cudaGraphAddKernelNode(out, g, deps.data(), deps.size(), &kp);
+}
+
+cudaError_t add_while(cudaGraphNode_t* out, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+                      cudaGraphConditionalHandle h, cudaGraph_t* body) {
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaError_t e = cudaGraphAddNode(out, g, deps.data(), deps.size(), &np);
+    if (e == cudaSuccess) *body = np.conditional.phGraph_out[0];
+    return e;
+}
+
+#define GK(call)                                                                        \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return fail(ctx, NTCFD_ECUDA, "graph build: %s: %s (line %d)", #call,        \
+                        cudaGetErrorString(e_), __LINE__);                              \
+    } while (0)
+
+template <class Tc>
+SorCoef<Tc> sor_coef(ntcfd_ctx* ctx);
+template <>
+SorCoef<double> sor_coef<double>(ntcfd_ctx* ctx) { return ctx->scd; }
+template <>
+SorCoef<float> sor_coef<float>(ntcfd_ctx* ctx) { return ctx->scf; }
+
+// The step graph:
+//   [K1 smag] -> K2 predictor -> K3a rhs -> begin -> WHILE(outer){ defect ->
+//   WHILE(inner){ c x (red, black) -> check } -> correct -> outer_check } ->
+//   K4 project -> K5 columns -> K5 total -> K6 x -> K6 y -> K6 z -> [divmax] -> end
+template <class Tc>
+int build_graph(ntcfd_ctx* ctx) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaGraph_t G;
+    GK(cudaGraphCreate(&G, 0));
+    ctx->graph = G;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    std::vector<cudaGraphNode_t> dep;
+    cudaGraphNode_t n;
+    if (P.LES) {
+        GK(add_kernel(&n, G, dep, k_smagorinsky, g3, b3, g, (const double*)ctx->u,
+                      (const double*)ctx->v, (const double*)ctx->w, ctx->nut, P.Cs,
+                      P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0));
+        dep = {n};
+    }
+    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
+                P.dt, 1. / P.Re, P.LES};
+    GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_rhs, g3, b3, g, ctx->scd, (const double*)ctx->u,
+                  (const double*)ctx->v, (const double*)ctx->w, (const double*)ctx->us,
+                  (const double*)ctx->vs, (const double*)ctx->ws, ctx->b, P.dt));
+    dep = {n};
+    cudaGraphConditionalHandle hout, hin;
+    GK(cudaGraphConditionalHandleCreate(&hout, G, 0, 0));
+    GK(add_kernel(&n, G, dep, k_sor_begin, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+    dep = {n};
+    cudaGraph_t outer;
+    GK(add_while(&n, G, dep, hout, &outer));
+    dep = {n};
+    {
+        GK(cudaGraphConditionalHandleCreate(&hin, outer, 0, 0));
+        std::vector<cudaGraphNode_t> od;
+        cudaGraphNode_t m;
+        Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+        GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
+                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, hin, 1));
+        od = {m};
+        cudaGraph_t inner;
+        GK(add_while(&m, outer, od, hin, &inner));
+        od = {m};
+        {
+            std::vector<cudaGraphNode_t> id;
+            cudaGraphNode_t s;
+            const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
+            const dim3 bs(kSweepBx, kSweepBy, 1);
+            const int half = (g.nx + 1) / 2;
+            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy, g.nz);
+            for (int sub = 0; sub < ctx->csweeps; ++sub) {
+                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy>, gs, bs, g, sc, eR,
+                              (const Tc*)eB, (const Tc*)dR, 0, P.omega, ctx->ctl, sub, P.itmax,
+                              ctx->cycle_len, ctx->slots));
+                id = {s};
+                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy>, gs, bs, g, sc, eB,
+                              (const Tc*)eR, (const Tc*)dB, 1, P.omega, ctx->ctl, sub, P.itmax,
+                              ctx->cycle_len, ctx->slots));
+                id = {s};
+            }
+            GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(1), ctx->ctl, ctx->slots,
+                          ctx->csweeps, P.itmax, ctx->cycle_len, P.zeta, hin));
+        }
+        GK(add_kernel(&m, outer, od, k_correct<Tc>, g3, b3, g, ctx->p, (const Tc*)eR, (const Tc*)eB));
+        od = {m};
+        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+    }
+    ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
+                ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
+    GK(add_kernel(&n, G, dep, k_project, dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk),
+                  dim3(32, 4, 1), g, pj));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_force_columns, dim3(296), dim3(256), g, (const double*)ctx->partZ,
+                  (const double*)ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_force_total<256>, dim3(1), dim3(256), g, (const double*)ctx->FXz,
+                  (const double*)ctx->FYz, P.lx, ctx->ctl, ctx->rec));
+    dep = {n};
+    BcArgs ba{};
+    ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+    std::memcpy(ba.bc, P.bc, sizeof ba.bc);
+    std::memcpy(ba.val, P.bc_value, sizeof ba.val);
+    ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
+    ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
+    GK(add_kernel(&n, G, dep, k_bc_x, dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), g, ba));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_bc_y, dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), g, ba));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_bc_z, dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), g, ba));
+    dep = {n};
+    if (P.diag_divergence) {
+        GK(add_kernel(&n, G, dep, k_divmax<256>, g3, b3, g, (const double*)ctx->u,
+                      (const double*)ctx->v, (const double*)ctx->w, ctx->divslot));
+        dep = {n};
+    }
+    const int fixed = 10 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0);
+    GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
+                  P.diag_divergence, fixed, ctx->csweeps));
+    GK(cudaGraphInstantiate(&ctx->exec, G, 0));
+    return 0;
+}
+
+int validate(const ntcfd_params* p, std::string* why) {
+    char b[256];
+    auto bad = [&](const char* m) { *why = m; return NTCFD_EINVAL; };
+    if (p->nx < 3 || p->ny < 3 || p->nz < 3) return bad("nx, ny, nz must be >= 3");
+    if (!(p->Re > 0) || !(p->dt > 0)) return bad("Re and dt must be positive");
+    if (!(p->omega > 0 && p->omega < 2)) return bad("omega must lie in (0, 2)");
+    if (p->itmax < 0) return bad("itmax must be >= 0");
+    if (!(p->zeta >= 0)) return bad("zeta must be >= 0");
+    if (p->precision != NTCFD_FP64 && p->precision != NTCFD_MIXED) return bad("precision must be NTCFD_FP64 or NTCFD_MIXED");
+    if (p->sor_order != NTCFD_SOR_REDBLACK)
+        return bad("the device solver is red-black SOR (sor_order = NTCFD_SOR_REDBLACK)");
+    if (p->scheme != NTCFD_QUICK_CENTRE) return bad("scheme must be NTCFD_QUICK_CENTRE");
+    if (p->smag_mode != NTCFD_SMAG_REF_ALIASED && p->smag_mode != NTCFD_SMAG_STAGGERED) return bad("bad smag_mode");
+    if (p->LES != 0 && p->LES != 1) return bad("LES must be 0 or 1");
+    if (p->check_every < 0 || p->mixed_cycle < 0) return bad("check_every and mixed_cycle must be >= 0");
+    for (int wl = 0; wl < 6; ++wl)
+        for (int c = 0; c < 3; ++c)
+            if (p->bc[wl][c] < 0 || p->bc[wl][c] > 3) return bad("bad boundary-condition kind");
+    for (int ax = 0; ax < 3; ++ax) {
+        const int lo = 2 * ax, hi = 2 * ax + 1;
+        bool any = false, all = true;
+        for (int c = 0; c < 3; ++c) {
+            for (int wl : {lo, hi}) {
+                const bool per = p->bc[wl][c] == NTCFD_BC_PERIODIC;
+                any = any || per;
+                all = all && per;
+            }
+        }
+        if (any && !all) {
+            snprintf(b, sizeof b, "periodic axis %d: both walls and all three components must be periodic", ax);
+            *why = b;
+            return NTCFD_EINVAL;
+        }
+    }
+    for (int q = 0; q < 6; ++q)
+        if (p->reserved[q] != 0) return bad("reserved fields must be zero");
+    return 0;
+}
+
+template <class T>
+void make_axis_tables(int n, const double* iD, const double* Ds, T* out /* 6 x (n+5) */,
+                      AxisTabs<T>* at, T** base_for_ptrs) {
+    // out layout: riD, rDs, As, Bs, Ac, Bc, each n+5 entries, entry q <-> index q-2
+    const int L = n + 5;
+    auto I = [&](const double* a, int i) { return a[i + 1]; };   // a(-1:n+2) from index 0
+    for (int q = 0; q < 6 * L; ++q) out[q] = T(0);
+    for (int i = -1; i <= n + 2; ++i) {
+        out[0 * L + i + 2] = (T)(1.0 / I(iD, i));
+        out[1 * L + i + 2] = (T)(1.0 / I(Ds, i));
+    }
+    for (int a = -1; a <= n + 1; ++a) {
+        const double h1 = I(iD, a + 1);
+        out[2 * L + a + 2] = (T)(0.125 * h1 * h1 / I(Ds, a));
+        out[3 * L + a + 2] = (T)(0.125 * h1 * h1 / I(Ds, a + 1));
+        const double H = I(Ds, a);
+        out[4 * L + a + 2] = (T)(0.125 * H * H / I(iD, a));
+        out[5 * L + a + 2] = (T)(0.125 * H * H / I(iD, a + 1));
+    }
+    (void)at;
+    (void)base_for_ptrs;
+}
+
+}  // namespace
+
+namespace {
+
+template <class Tc>
+int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    float ms = 0.0f;
+    auto timed = [&](auto&& launch, float* dst, int per) -> int {
+        launch();  // warm-up
+        CK(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int r = 0; r < reps; ++r) launch();
+        CK(cudaEventRecord(ctx->ev1, ctx->stream));
+        CK(cudaEventSynchronize(ctx->ev1));
+        CK(cudaGetLastError());
+        CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        *dst = ms / (float)(reps * per);
+        return 0;
+    };
+    int rc;
+    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
+                P.dt, 1. / P.Re, P.LES};
+    if ((rc = timed([&] {
+             if (P.LES)
+                 k_smagorinsky<<<g3, b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
+                                                           P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
+             k_predictor<double><<<g3, b3, 0, ctx->stream>>>(g, ctx->tpd, pa);
+         }, &out->predictor_ms, 1)))
+        return rc;
+    if ((rc = timed([&] {
+             k_rhs<<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs,
+                                               ctx->ws, ctx->b, P.dt);
+         }, &out->rhs_ms, 1)))
+        return rc;
+    Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+    if ((rc = timed([&] {
+             k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
+                                                      ctx->ctl, 0, 0);
+         }, &out->defect_ms, 1)))
+        return rc;
+    const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
+    const dim3 bs(kSweepBx, kSweepBy, 1);
+    const int half = (g.nx + 1) / 2;
+    const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy, g.nz);
+    const int big = 1 << 30;
+    if ((rc = timed([&] {
+             k_sweep<Tc, kSweepBx * kSweepBy><<<gs, bs, 0, ctx->stream>>>(
+                 g, sc, eR, eB, dR, 0, P.omega, ctx->ctl, 0, big, big, ctx->slots);
+             k_sweep<Tc, kSweepBx * kSweepBy><<<gs, bs, 0, ctx->stream>>>(
+                 g, sc, eB, eR, dB, 1, P.omega, ctx->ctl, 0, big, big, ctx->slots);
+         }, &out->sweep_ms, 2)))
+        return rc;
+    // K4 on the predicted velocity in place (us/vs/ws are rewritten every step)
+    ProjArgs pj{ctx->us, ctx->vs, ctx->ws, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
+                ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
+    if ((rc = timed([&] {
+             k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0,
+                         ctx->stream>>>(g, pj);
+         }, &out->project_ms, 1)))
+        return rc;
+    // K6 is idempotent on the state; the saved faces go to scratch here
+    BcArgs ba{};
+    ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+    std::memcpy(ba.bc, P.bc, sizeof ba.bc);
+    std::memcpy(ba.val, P.bc_value, sizeof ba.val);
+    double* junk = ctx->outbuf;
+    const size_t nxy = (size_t)g.nx * g.ny, nxz = (size_t)g.nx * g.nz;
+    ba.faceW = junk; ba.faceE = junk + (size_t)g.ny * g.nz; ba.faceS = ba.faceE + (size_t)g.ny * g.nz;
+    ba.faceN = ba.faceS + nxz; ba.faceB = ba.faceN + nxz; ba.faceF = ba.faceB + nxy;
+    if ((rc = timed([&] {
+             k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+             k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+             k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+         }, &out->bc_ms, 1)))
+        return rc;
+    return 0;
+}
+
+}  // namespace
+
+// =====================================================================  ABI
+extern "C" {
+
+void ntcfd_default_params(ntcfd_params* p) {
+    std::memset(p, 0, sizeof *p);
+    p->nx = p->ny = p->nz = 40;
+    p->Re = 10.0;
+    p->dt = (double)1.0e-3f;      // real*8 parameter initialised from a default-real literal
+    p->omega = 1.5;
+    p->zeta = (double)1.e-4f;
+    p->itmax = 3000;
+    p->LES = 0;
+    p->Cs = (double)0.18f;
+    p->scheme = NTCFD_QUICK_CENTRE;
+    p->precision = NTCFD_FP64;
+    p->sor_order = NTCFD_SOR_REDBLACK;
+    p->smag_mode = NTCFD_SMAG_REF_ALIASED;
+    p->check_every = 1;
+    for (int wl = 0; wl < 6; ++wl)
+        for (int c = 0; c < 3; ++c) {
+            p->bc[wl][c] = NTCFD_BC_NOSLIP;
+            p->bc_value[wl][c] = 1.0;
+        }
+    p->bc[NTCFD_NORTH][2] = NTCFD_BC_DIRICHLET;   // NorthWall_w = 'Dirichlet'
+    p->lx = 1.0;
+}
+
+int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
+    if (!prm || !out) return NTCFD_EINVAL;
+    *out = nullptr;
+    std::string why;
+    ntcfd_ctx* ctx = new ntcfd_ctx();
+    if (int rc = validate(prm, &why)) {
+        // a context is still returned so that ntcfd_last_error can explain the failure
+        ctx->err = why;
+        *out = ctx;
+        return rc;
+    }
+    ctx->prm = *prm;
+    ntcfd_params& P = ctx->prm;
+    if (P.check_every == 0) P.check_every = 1;
+    ctx->csweeps = P.check_every;
+    int cl = P.mixed_cycle > 0 ? P.mixed_cycle : P.itmax;
+    if (P.mixed_cycle > 0 && cl % ctx->csweeps) cl += ctx->csweeps - cl % ctx->csweeps;
+    ctx->cycle_len = cl > 0 ? cl : 1;
+    *out = ctx;
+    CK(cudaSetDevice(P.device));
+    CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&ctx->ev0));
+    CK(cudaEventCreate(&ctx->ev1));
+    Geom& g = ctx->g;
+    g.nx = P.nx; g.ny = P.ny; g.nz = P.nz;
+    g.px = ((P.nx + 10) + 7) & ~7;
+    g.py = P.ny + 4;
+    g.pz = (long long)g.px * g.py;
+    g.mxp = ((((P.nx + 3) >> 1) + 1) + 7) & ~7;
+    g.mz = (long long)g.mxp * g.py;
+    ctx->nat_elems = (size_t)g.pz * (P.nz + 4);
+    ctx->spl_elems = (size_t)g.mz * (P.nz + 4);
+    const size_t N = ctx->nat_elems;
+    int rc;
+    double** nat[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->us, &ctx->vs, &ctx->ws, &ctx->b, &ctx->eta};
+    for (double** a : nat)
+        if ((rc = dalloc(ctx, a, N))) return rc;
+    if (P.LES && (rc = dalloc(ctx, &ctx->nut, N))) return rc;
+    const size_t esz = P.precision == NTCFD_MIXED ? sizeof(float) : sizeof(double);
+    void** spl[] = {&ctx->eR, &ctx->eB, &ctx->dR, &ctx->dB};
+    for (void** a : spl) {
+        char* q;
+        if ((rc = dalloc(ctx, &q, ctx->spl_elems * esz))) return rc;
+        *a = q;
+    }
+    ctx->nchunk = (P.nz + kProjKc - 1) / kProjKc;
+    const size_t cols = (size_t)P.nx * P.ny;
+    if ((rc = dalloc(ctx, &ctx->partZ, cols * ctx->nchunk))) return rc;
+    if ((rc = dalloc(ctx, &ctx->partY, cols * ctx->nchunk))) return rc;
+    if ((rc = dalloc(ctx, &ctx->FXz, cols))) return rc;
+    if ((rc = dalloc(ctx, &ctx->FYz, cols))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceW, (size_t)P.ny * P.nz))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceE, (size_t)P.ny * P.nz))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceS, (size_t)P.nx * P.nz))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceN, (size_t)P.nx * P.nz))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceB, (size_t)P.nx * P.ny))) return rc;
+    if ((rc = dalloc(ctx, &ctx->faceF, (size_t)P.nx * P.ny))) return rc;
+    if ((rc = dalloc(ctx, &ctx->outbuf, 4 * (size_t)P.nx * P.ny * P.nz))) return rc;
+    if ((rc = dalloc(ctx, &ctx->ctl, 1))) return rc;
+    if ((rc = dalloc(ctx, &ctx->slots, 64))) return rc;
+    if ((rc = dalloc(ctx, &ctx->divslot, 1))) return rc;
+    if ((rc = dalloc(ctx, &ctx->coordbuf, (size_t)(P.ny + 5) + (P.nz + 5) + 8))) return rc;
+    ctx->coordY = ctx->coordbuf + 1;                  // Y[j] valid for j = -1..ny+3
+    ctx->coordZ = ctx->coordbuf + (P.ny + 5) + 4 + 1;
+    if (ctx->csweeps > 64) return fail(ctx, NTCFD_EINVAL, "check_every must be <= 64");
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+void ntcfd_destroy(ntcfd_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->stream) cudaSetDevice(ctx->prm.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    for (void* q : ctx->allocs) cudaFree(q);
+    if (ctx->rec) cudaFree(ctx->rec);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* ntcfd_last_error(const ntcfd_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+double ntcfd_time(const ntcfd_ctx* ctx) { return ctx ? ctx->time : 0.0; }
+
+int ntcfd_set_metrics(ntcfd_ctx* ctx, const double* iDx, const double* Dxs, const double* iDy,
+                      const double* Dys, const double* iDz, const double* Dzs) {
+    DEV();
+    if (!iDx || !Dxs || !iDy || !Dys || !iDz || !Dzs) return fail(ctx, NTCFD_EINVAL, "null metric array");
+    Geom& g = ctx->g;
+    const int n[3] = {g.nx, g.ny, g.nz};
+    const double* iD[3] = {iDx, iDy, iDz};
+    const double* Ds[3] = {Dxs, Dys, Dzs};
+    for (int ax = 0; ax < 3; ++ax)
+        for (int i = 0; i < n[ax] + 4; ++i)
+            if (!(iD[ax][i] > 0) || !(Ds[ax][i] > 0))
+                return fail(ctx, NTCFD_EINVAL, "metric %d index %d is not positive", ax, i - 1);
+    // double tables: iD, Ds, riD, rDs (4 per axis) + cE..cB (6) + predictor tables (6 per axis)
+    int L[3];
+    size_t tot = 0;
+    for (int ax = 0; ax < 3; ++ax) { L[ax] = n[ax] + 5; tot += (size_t)L[ax] * (4 + 2 + 6); }
+    std::vector<double> hd(tot, 0.0);
+    std::vector<float> hf(tot, 0.0f);
+    size_t off = 0;
+    std::vector<size_t> offs;
+    auto take = [&](int len) { offs.push_back(off); size_t o = off; off += len; return o; };
+    size_t o_iD[3], o_Ds[3], o_riD[3], o_rDs[3], o_c1[3], o_c2[3], o_tab[3];
+    for (int ax = 0; ax < 3; ++ax) {
+        const int Lx = L[ax];
+        o_iD[ax] = take(Lx); o_Ds[ax] = take(Lx); o_riD[ax] = take(Lx); o_rDs[ax] = take(Lx);
+        o_c1[ax] = take(Lx); o_c2[ax] = take(Lx);
+        o_tab[ax] = take(6 * Lx);
+        for (int i = -1; i <= n[ax] + 2; ++i) {
+            const double h = iD[ax][i + 1], H = Ds[ax][i + 1];
+            hd[o_iD[ax] + i + 2] = h;
+            hd[o_Ds[ax] + i + 2] = H;
+            hd[o_riD[ax] + i + 2] = 1.0 / h;
+            hd[o_rDs[ax] + i + 2] = 1.0 / H;
+        }
+        // SOR coefficients over the volume: c+(i) = 1/(iD(i) Ds(i)), c-(i) = 1/(iD(i) Ds(i-1))
+        for (int i = 0; i <= n[ax] + 2; ++i) {
+            hd[o_c1[ax] + i + 2] = 1.0 / (iD[ax][i + 1] * Ds[ax][i + 1]);
+            hd[o_c2[ax] + i + 2] = 1.0 / (iD[ax][i + 1] * Ds[ax][i]);
+        }
+        make_axis_tables<double>(n[ax], iD[ax], Ds[ax], hd.data() + o_tab[ax], nullptr, nullptr);
+    }
+    for (size_t q = 0; q < tot; ++q) hf[q] = (float)hd[q];
+    if (!ctx->tabd) {
+        int rc;
+        if ((rc = dalloc(ctx, &ctx->tabd, tot))) return rc;
+        if ((rc = dalloc(ctx, &ctx->tabf, tot))) return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->tabd, hd.data(), tot * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->tabf, hf.data(), tot * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    const double* D = ctx->tabd + 2;
+    const float* F = ctx->tabf + 2;
+    g.iDx = D + o_iD[0]; g.Dxs = D + o_Ds[0]; g.iDy = D + o_iD[1]; g.Dys = D + o_Ds[1];
+    g.iDz = D + o_iD[2]; g.Dzs = D + o_Ds[2];
+    g.riDx = D + o_riD[0]; g.rDxs = D + o_rDs[0]; g.riDy = D + o_riD[1]; g.rDys = D + o_rDs[1];
+    g.riDz = D + o_riD[2]; g.rDzs = D + o_rDs[2];
+    g.cE = D + o_c1[0]; g.cW = D + o_c2[0]; g.cN = D + o_c1[1]; g.cS = D + o_c2[1];
+    g.cF = D + o_c1[2]; g.cB = D + o_c2[2];
+    g.cEf = F + o_c1[0]; g.cWf = F + o_c2[0]; g.cNf = F + o_c1[1]; g.cSf = F + o_c2[1];
+    g.cFf = F + o_c1[2]; g.cBf = F + o_c2[2];
+    ctx->scd = SorCoef<double>{g.cE, g.cW, g.cN, g.cS, g.cF, g.cB};
+    ctx->scf = SorCoef<float>{g.cEf, g.cWf, g.cNf, g.cSf, g.cFf, g.cBf};
+    for (int ax = 0; ax < 3; ++ax) {
+        const int Lx = L[ax];
+        const double* tb = D + o_tab[ax];
+        const float* tf = F + o_tab[ax];
+        ctx->tpd.ax[ax] = AxisTabs<double>{tb, tb + Lx, tb + 2 * Lx, tb + 3 * Lx, tb + 4 * Lx, tb + 5 * Lx};
+        ctx->tpf.ax[ax] = AxisTabs<float>{tf, tf + Lx, tf + 2 * Lx, tf + 3 * Lx, tf + 4 * Lx, tf + 5 * Lx};
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->metrics_set = true;
+    if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    return 0;
+}
+
+int ntcfd_set_coords(ntcfd_ctx* ctx, const double* X, const double* Y, const double* Z) {
+    DEV();
+    if (!Y || !Z) return fail(ctx, NTCFD_EINVAL, "null coordinate array");
+    (void)X;
+    const int ny = ctx->g.ny, nz = ctx->g.nz;
+    CK(cudaMemcpyAsync(ctx->coordbuf, Y, (ny + 5) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->coordbuf + (ny + 5) + 4, Z, (nz + 5) * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->coords_set = true;
+    return 0;
+}
+
+static int copy_halo(ntcfd_ctx* ctx, double* dev, const double* host, bool to_dev) {
+    const Geom& g = ctx->g;
+    double* d0 = dev + nat(g, -1, -1, -1);
+    const size_t w = (size_t)(g.nx + 4) * sizeof(double);
+    const size_t h = (size_t)(g.ny + 4) * (g.nz + 4);
+    if (to_dev)
+        CK(cudaMemcpy2DAsync(d0, g.px * sizeof(double), host, w, w, h, cudaMemcpyHostToDevice, ctx->stream));
+    else
+        CK(cudaMemcpy2DAsync((void*)host, w, d0, g.px * sizeof(double), w, h, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return 0;
+}
+
+int ntcfd_set_mask(ntcfd_ctx* ctx, const double* eta) {
+    DEV();
+    if (!eta) return fail(ctx, NTCFD_EINVAL, "null ETA");
+    int rc = copy_halo(ctx, ctx->eta, eta, true);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_get_mask(ntcfd_ctx* ctx, double* eta) {
+    DEV();
+    if (!eta) return fail(ctx, NTCFD_EINVAL, "null ETA");
+    int rc = copy_halo(ctx, ctx->eta, eta, false);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_set_state(ntcfd_ctx* ctx, const double* u, const double* v, const double* w, const double* p) {
+    DEV();
+    if (!u || !v || !w || !p) return fail(ctx, NTCFD_EINVAL, "null state array");
+    int rc;
+    if ((rc = copy_halo(ctx, ctx->u, u, true))) return rc;
+    if ((rc = copy_halo(ctx, ctx->v, v, true))) return rc;
+    if ((rc = copy_halo(ctx, ctx->w, w, true))) return rc;
+    if ((rc = copy_halo(ctx, ctx->p, p, true))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_get_state(ntcfd_ctx* ctx, double* u, double* v, double* w, double* p) {
+    DEV();
+    int rc;
+    if (u && (rc = copy_halo(ctx, ctx->u, u, false))) return rc;
+    if (v && (rc = copy_halo(ctx, ctx->v, v, false))) return rc;
+    if (w && (rc = copy_halo(ctx, ctx->w, w, false))) return rc;
+    if (p && (rc = copy_halo(ctx, ctx->p, p, false))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_apply_bc(ntcfd_ctx* ctx) {
+    DEV();
+    const Geom& g = ctx->g;
+    BcArgs ba{};
+    ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+    std::memcpy(ba.bc, ctx->prm.bc, sizeof ba.bc);
+    std::memcpy(ba.val, ctx->prm.bc_value, sizeof ba.val);
+    ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
+    ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
+    k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_get_output(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
+    DEV();
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "metrics not set");
+    const Geom& g = ctx->g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    double* o = ctx->outbuf;
+    const dim3 b3(32, 4, 2);
+    k_centre<<<grid3(g, b3), b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->p, ctx->faceW,
+                                                   ctx->faceE, ctx->faceS, ctx->faceN, ctx->faceB,
+                                                   ctx->faceF, o, o + n, o + 2 * n, o + 3 * n);
+    CK(cudaGetLastError());
+    double* dst[4] = {pre, uc, vc, wc};
+    for (int q = 0; q < 4; ++q)
+        if (dst[q])
+            CK(cudaMemcpyAsync(dst[q], o + q * n, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
+    DEV();
+    if (nsteps < 0) return fail(ctx, NTCFD_EINVAL, "nsteps < 0");
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_step");
+    if (nsteps == 0) return 0;
+    if (nsteps > ctx->rec_cap) {
+        // the graph holds the record pointer: grow the record buffer, then rebuild
+        const int cap = std::max(nsteps, 1024);
+        if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+        if (ctx->rec) cudaFree(ctx->rec);
+        ctx->rec = nullptr;
+        ctx->rec_cap = 0;
+        CK(cudaMalloc(&ctx->rec, sizeof(StepRec) * cap));
+        ctx->rec_cap = cap;
+    }
+    if (!ctx->exec) {
+        const int rc = ctx->prm.precision == NTCFD_MIXED ? build_graph<float>(ctx) : build_graph<double>(ctx);
+        if (rc) return rc;
+    }
+    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(ctx->exec, ctx->stream));
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    std::vector<StepRec> rec(nsteps);
+    CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    int status = 0;
+    for (int s = 0; s < nsteps; ++s) {
+        ctx->time = ctx->time + ctx->prm.dt;   // main.f90:271
+        if (rec[s].nonfinite) status = NTCFD_ENONFINITE;
+        else if (!rec[s].converged && status == 0) status = NTCFD_NOT_CONVERGED;
+        if (info) {
+            ntcfd_step_info& I = info[s];
+            std::memset(&I, 0, sizeof I);
+            I.sor_iters = rec[s].sor_iters;
+            I.converged = rec[s].converged;
+            I.sor_last_change = rec[s].last_change;
+            I.cDrag = rec[s].cdrag;
+            I.cLift = rec[s].clift;
+            I.div_max = rec[s].divmax;
+            I.dc_cycles = rec[s].cycles;
+            I.launches = rec[s].launches;
+        }
+    }
+    if (status == NTCFD_ENONFINITE) fail(ctx, status, "non-finite value in the SOR solve");
+    else if (status == NTCFD_NOT_CONVERGED) fail(ctx, status, "SOR stopped at itmax in at least one step");
+    return status;
+}
+
+int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return NTCFD_EINVAL;
+    *ms = ctx->last_ms;
+    return 0;
+}
+
+int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
+    DEV();
+    if (!out || reps < 1) return fail(ctx, NTCFD_EINVAL, "bad arguments");
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "metrics not set");
+    std::memset(out, 0, sizeof *out);
+    return ctx->prm.precision == NTCFD_MIXED ? time_kernels_t<float>(ctx, reps, out)
+                                            : time_kernels_t<double>(ctx, reps, out);
+}
+
+// ------------------------------------------------------------------ masks
+int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r) {
+    DEV();
+    if (!ctx->metrics_set || !ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "metrics and coordinates first");
+    const Geom& g = ctx->g;
+    double* eta1 = ctx->outbuf;  // scratch: nz*ny
+    k_cylinder<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+        g.ny, g.nz, ctx->coordY, ctx->coordZ, g.iDx, g.iDy, g.iDz, zc, yc, r, eta1);
+    const dim3 b3(32, 4, 2);
+    k_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), b3, 0, ctx->stream>>>(
+        g, eta1, ctx->eta);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* ay_in, int npts,
+                             double aoa, double zc, double yc, int* ties_out) {
+    DEV();
+    if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
+    if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    const Geom& g = ctx->g;
+    // airfoil.f90:597-611 on the host: shift by the quarter chord, rotate by
+    // -AOA (ay uses the already rotated az, as in the reference), translate.
+    std::vector<double> az(az_in, az_in + npts), ay(ay_in, ay_in + npts);
+    const double PI = 4.0 * std::atan(1.0);
+    for (int i = 0; i < npts; ++i) {
+        az[i] = az[i] - 0.25;
+        az[i] = std::cos((-aoa) * PI / 180) * az[i] - std::sin((-aoa) * PI / 180) * ay[i];
+        ay[i] = std::sin((-aoa) * PI / 180) * az[i] + std::cos((-aoa) * PI / 180) * ay[i];
+        az[i] = az[i] + zc;
+        ay[i] = ay[i] + yc;
+        az[i] = az[i] + 0.25;
+    }
+    // node coordinates back on the host for the A, B, C, E search (airfoil.f90:615-654)
+    std::vector<double> Y(g.ny + 5), Z(g.nz + 5);
+    CK(cudaMemcpyAsync(Y.data(), ctx->coordbuf, (g.ny + 5) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Z.data(), ctx->coordbuf + (g.ny + 5) + 4, (g.nz + 5) * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    auto Yf = [&](int j) { return Y[j + 1]; };
+    auto Zf = [&](int k) { return Z[k + 1]; };
+    double miny = ay[0], maxy = ay[0], minz = az[0], maxz = az[0];
+    for (int i = 1; i < npts; ++i) {
+        miny = std::min(miny, ay[i]); maxy = std::max(maxy, ay[i]);
+        minz = std::min(minz, az[i]); maxz = std::max(maxz, az[i]);
+    }
+    int A = 0, B = 0, C = 0, E = 0;
+    for (int j = 1; j <= g.ny; ++j) if (Yf(j) > miny) { A = j - 1; break; }
+    for (int j = 1; j <= g.ny; ++j) if (Yf(j) > maxy) { B = j; break; }
+    for (int k = 1; k <= g.nz; ++k) if (Zf(k) > minz) { C = k - 1; break; }
+    for (int k = 1; k <= g.nz; ++k) if (Zf(k) > maxz) { E = k; break; }
+    // device work buffers
+    double* daz = nullptr;
+    int* dint = nullptr;
+    const size_t cells = (size_t)g.ny * g.nz;
+    CK(cudaMalloc(&daz, sizeof(double) * 2 * npts));
+    CK(cudaMalloc(&dint, sizeof(int) * (2 * cells + 1)));
+    double* day = daz + npts;
+    int* points = dint;
+    int* list = dint + cells;
+    int* ties = dint + 2 * cells;
+    CK(cudaMemcpyAsync(daz, az.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(day, ay.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemsetAsync(dint, 0, sizeof(int) * (2 * cells + 1), ctx->stream));
+    double* eta1 = ctx->outbuf;
+    k_ray_main<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+        g.ny, g.nz, ctx->coordY, ctx->coordZ, daz, day, npts, eta1, ties);
+    k_ray_points<<<(npts + 127) / 128, 128, 0, ctx->stream>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, daz,
+                                                                day, npts, A, B, C, E, points);
+    std::vector<int> hp(cells);
+    CK(cudaMemcpyAsync(hp.data(), points, sizeof(int) * cells, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> hl;
+    for (size_t q = 0; q < cells; ++q)
+        if (hp[q]) hl.push_back((int)q);
+    if (!hl.empty()) {
+        CK(cudaMemcpyAsync(list, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice, ctx->stream));
+        k_ray_sub<256><<<(unsigned)hl.size(), 256, 0, ctx->stream>>>(g.nz, ctx->coordY, ctx->coordZ, daz,
+                                                                    day, npts, list, eta1, ties);
+    }
+    const dim3 b3(32, 4, 2);
+    k_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), b3, 0, ctx->stream>>>(
+        g, eta1, ctx->eta);
+    int hties = 0;
+    CK(cudaMemcpyAsync(&hties, ties, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(daz);
+    cudaFree(dint);
+    if (ties_out) *ties_out = hties;
+    if (hties)
+        return fail(ctx, NTCFD_EINVAL,
+                    "%d exact vertex/grid ties: the reference resolves them by moving the grid", hties);
+    return 0;
+}
+
+}  // extern "C"

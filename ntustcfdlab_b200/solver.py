@@ -1,0 +1,207 @@
+"""Host-side driver of the B200 time step, mirroring the reference's
+initialisation and step sequence (main.f90:77-110 then the loop body
+main.f90:209-271) over the C-ABI of ``include/ntcfd.h``.
+
+    grid = gridder_equal(nx, ny, nz, lx, ly, lz)       # reading_data + gridder_equal
+    s = Solver(params, grid)                           # initial_conditions (all zero)
+    s.boundary_conditions()                            # main.f90:100
+    s.build_mask_polygon(az, ay, aoa, zc, yc)          # RayCasting, main.f90:109-110
+    info = s.step(nsteps)                              # the loop body
+    pre, uc, vc, wc = s.get_output()                   # filereachtime fields
+
+Arrays are numpy float64 in Fortran order: halo arrays have shape
+(nx+4, ny+4, nz+4), array index i+1 for Fortran index i (-1..n+2).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import abi
+from .abi import NtcfdParams, NtcfdStepInfo, dptr
+
+
+class NtcfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"ntcfd error {code}: {msg}")
+        self.code = code
+
+
+def _grid_arrays(nx, ny, nz):
+    X, Y, Z = np.zeros(nx + 5), np.zeros(ny + 5), np.zeros(nz + 5)
+    m = [np.zeros(n + 4) for n in (nx, nx, ny, ny, nz, nz)]
+    return X, Y, Z, m
+
+
+def _grid_dict(X, Y, Z, m):
+    return dict(X=X, Y=Y, Z=Z, iDx=m[0], Dxs=m[1], iDy=m[2], Dys=m[3], iDz=m[4], Dzs=m[5])
+
+
+def gridder_equal(nx, ny, nz, lx=1.0, ly=1.0, lz=1.0) -> dict:
+    """reading_data + gridder_equal (reading_data.f90:26-30, gridder.f90:228-327)."""
+    lib = abi.load_library()
+    X, Y, Z, m = _grid_arrays(nx, ny, nz)
+    lib.ntcfd_gridder_equal(nx, ny, nz, lx, ly, lz, dptr(X), dptr(Y), dptr(Z), *[dptr(a) for a in m])
+    return _grid_dict(X, Y, Z, m)
+
+
+def gridder_unequal(nx, ny, nz, lx, ly, lz, band) -> dict:
+    """reading_data + gridder_Unequal (reading_data.f90:6-23, gridder.f90:1-157).
+    band = (GridderXc, GridderYc, GridderZc, nxSml, nySml, nyMid, nzSml, nzMid,
+            lxSml, lySml, lyMid, lzSml, lzMid)."""
+    lib = abi.load_library()
+    X, Y, Z, m = _grid_arrays(nx, ny, nz)
+    b = np.asarray(band, dtype=np.float64)
+    lib.ntcfd_gridder_unequal(nx, ny, nz, lx, ly, lz, dptr(b), dptr(X), dptr(Y), dptr(Z),
+                              *[dptr(a) for a in m])
+    return _grid_dict(X, Y, Z, m)
+
+
+def naca4_polygon(t: float, npts: int = 256):
+    """Closed analytic NACA 4-digit symmetric section (chord 1), ordered like
+    NACA0012.DAT (LE -> upper -> TE -> lower -> LE)."""
+    lib = abi.load_library()
+    z, y = np.zeros(2 * npts), np.zeros(2 * npts)
+    n = lib.ntcfd_naca4_polygon(t, npts, dptr(z), dptr(y))
+    return z[:n], y[:n]
+
+
+def circle_polygon(r: float, npts: int = 128):
+    lib = abi.load_library()
+    z, y = np.zeros(npts + 1), np.zeros(npts + 1)
+    n = lib.ntcfd_circle_polygon(r, npts, dptr(z), dptr(y))
+    return z[:n], y[:n]
+
+
+class Solver:
+    """One device-resident grid (an ``ntcfd_ctx``)."""
+
+    def __init__(self, params: NtcfdParams, grid: dict):
+        self.lib = abi.load_library()
+        self.prm = params
+        self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
+        h = ctypes.c_void_p()
+        rc = self.lib.ntcfd_create(ctypes.byref(params), ctypes.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self._err()
+            self.close()
+            raise NtcfdError(rc, msg)
+        self.grid = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in grid.items()}
+        g = self.grid
+        self._check(self.lib.ntcfd_set_metrics(self.h, dptr(g["iDx"]), dptr(g["Dxs"]), dptr(g["iDy"]),
+                                               dptr(g["Dys"]), dptr(g["iDz"]), dptr(g["Dzs"])))
+        self._check(self.lib.ntcfd_set_coords(self.h, dptr(g["X"]), dptr(g["Y"]), dptr(g["Z"])))
+
+    # ------------------------------------------------------------ plumbing
+    def _err(self) -> str:
+        if not self.h:
+            return "no context"
+        m = self.lib.ntcfd_last_error(self.h)
+        return m.decode() if m else ""
+
+    def _check(self, rc: int, allow_warning: bool = False) -> int:
+        if rc < 0 or (rc > 0 and not allow_warning):
+            raise NtcfdError(rc, self._err())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None) and self.h.value:
+            self.lib.ntcfd_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def halo_shape(self):
+        return (self.nx + 4, self.ny + 4, self.nz + 4)
+
+    @property
+    def inner_shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    def _halo(self):
+        return np.zeros(self.halo_shape, dtype=np.float64, order="F")
+
+    # ------------------------------------------------------------ state
+    def set_state(self, u, v, w, p):
+        arrs = [np.asfortranarray(a, dtype=np.float64) for a in (u, v, w, p)]
+        for a in arrs:
+            if a.shape != self.halo_shape:
+                raise ValueError(f"state arrays must have shape {self.halo_shape}")
+        self._check(self.lib.ntcfd_set_state(self.h, *[dptr(a) for a in arrs]))
+
+    def get_state(self):
+        arrs = [self._halo() for _ in range(4)]
+        self._check(self.lib.ntcfd_get_state(self.h, *[dptr(a) for a in arrs]))
+        return tuple(arrs)
+
+    def set_mask(self, eta):
+        eta = np.asfortranarray(eta, dtype=np.float64)
+        self._check(self.lib.ntcfd_set_mask(self.h, dptr(eta)))
+
+    def get_mask(self):
+        a = self._halo()
+        self._check(self.lib.ntcfd_get_mask(self.h, dptr(a)))
+        return a
+
+    def build_mask_polygon(self, az, ay, aoa_deg, zc, yc) -> int:
+        """RayCasting (airfoil.f90:580-915) on the device."""
+        az = np.ascontiguousarray(az, dtype=np.float64)
+        ay = np.ascontiguousarray(ay, dtype=np.float64)
+        ties = ctypes.c_int(0)
+        self._check(self.lib.ntcfd_build_mask_polygon(self.h, dptr(az), dptr(ay), len(az), aoa_deg,
+                                                      zc, yc, ctypes.byref(ties)))
+        return ties.value
+
+    def build_mask_cylinder(self, zc, yc, r):
+        """DFIB_Cylinder (DFIB.f90:74-145) on the device."""
+        self._check(self.lib.ntcfd_build_mask_cylinder(self.h, zc, yc, r))
+
+    def boundary_conditions(self):
+        """boundary_conditions() (boundary_conditions.f90:13-374)."""
+        self._check(self.lib.ntcfd_apply_bc(self.h))
+
+    initial_boundary_conditions = boundary_conditions
+
+    def get_output(self):
+        """(pre, uc, vc, wc), each (nx, ny, nz) Fortran order."""
+        arrs = [np.zeros(self.inner_shape, dtype=np.float64, order="F") for _ in range(4)]
+        self._check(self.lib.ntcfd_get_output(self.h, *[dptr(a) for a in arrs]))
+        return tuple(arrs)
+
+    def step(self, nsteps: int = 1):
+        """Runs the loop body nsteps times; returns (list of NtcfdStepInfo, status).
+        status is 0 or NTCFD_NOT_CONVERGED; errors raise."""
+        info = (NtcfdStepInfo * max(nsteps, 1))()
+        rc = self.lib.ntcfd_step(self.h, nsteps, info)
+        self._check(rc, allow_warning=True)
+        return list(info)[:nsteps], rc
+
+    @property
+    def time(self) -> float:
+        return self.lib.ntcfd_time(self.h)
+
+    def last_step_ms(self) -> float:
+        """Device time (CUDA events on the context's stream) of the last step() call."""
+        ms = ctypes.c_float(0.0)
+        self._check(self.lib.ntcfd_last_step_ms(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def time_kernels(self, reps: int = 20) -> dict:
+        """Average device time (ms) of standalone launches of the step kernels."""
+        t = abi.NtcfdKernelTimes()
+        self._check(self.lib.ntcfd_time_kernels(self.h, reps, ctypes.byref(t)))
+        return {n: getattr(t, n) for n in ("predictor_ms", "rhs_ms", "defect_ms", "sweep_ms",
+                                           "project_ms", "bc_ms")}

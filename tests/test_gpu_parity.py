@@ -1,0 +1,253 @@
+"""GPU parity: the CUDA step (through the C-ABI) against the CPU oracle on
+the same inputs.
+
+Tolerances: the device evaluates the reference's algebra with tabulated
+reciprocals and fused multiply-adds, so FP64 results agree to rounding,
+not bit for bit.  Red-black FP64 vs the oracle's red-black mode with the
+same sweep counts: relative L2 <= 1e-12 per field.  Boundary conditions and
+masks are pure copies / counts and must match exactly.
+"""
+import numpy as np
+import pytest
+
+from conftest import interior, rel_l2
+from ntustcfdlab_b200 import abi
+from ntustcfdlab_b200.abi import (FP64, MIXED, SMAG_REF_ALIASED, SMAG_STAGGERED, SOR_LEX,
+                                  SOR_REDBLACK, f4, make_params, params_copy)
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("u", "v", "w", "p")
+
+
+def _solver(params, grid):
+    from ntustcfdlab_b200.solver import Solver
+    return Solver(params, grid)
+
+
+def _random_state(shape, seed, scale=0.3):
+    rng = np.random.default_rng(seed)
+    return [np.asfortranarray(scale * rng.standard_normal(shape)) for _ in range(4)]
+
+
+def _pair(orc, params, grid, state=None, oracle_sor=SOR_REDBLACK):
+    """A GPU solver and an oracle with identical initial state after the
+    initial boundary conditions (main.f90:92-100)."""
+    s = _solver(params, grid)
+    o = orc.Oracle(params_copy(params, sor_order=oracle_sor), grid)
+    o.initial_conditions()
+    if state is not None:
+        s.set_state(*state)
+        for k, a in zip(FIELDS, state):
+            o.set(k, a)
+    s.boundary_conditions()
+    o.boundary_conditions()
+    return s, o
+
+
+def _compare(s, o, tol, fields=FIELDS):
+    got = dict(zip(FIELDS, s.get_state()))
+    out = {}
+    for k in fields:
+        out[k] = rel_l2(interior(got[k]), interior(o.get(k)))
+        assert out[k] <= tol, (k, out[k])
+    return out
+
+
+BCS = {
+    "cavity": {"North": ("Dirichlet", "no-slip", "no-slip")},
+    "mixed": {"West": ("no-slip", "Neumann", "Dirichlet"), "East": ("Neumann", "no-slip", "Neumann"),
+              "South": ("Neumann", "no-slip", "Dirichlet"), "North": ("Dirichlet", "Neumann", "no-slip"),
+              "Back": ("Dirichlet", "Neumann", "Dirichlet"), "Front": ("Neumann", "Neumann", "Neumann")},
+    "periodic_x": {"West": ("periodic",) * 3, "East": ("periodic",) * 3,
+                   "Back": ("Dirichlet", "Dirichlet", "Dirichlet"), "Front": ("Neumann",) * 3,
+                   "South": ("Neumann",) * 3, "North": ("Neumann",) * 3},
+}
+
+
+@pytest.mark.parametrize("bcname", list(BCS))
+def test_boundary_conditions_exact(orc, bcname):
+    n = (13, 11, 9)
+    g = orc.gridder_equal(*n, 1.0, 1.0, 1.0)
+    p = make_params(*n, Re=100.0, dt=1e-3, bc=BCS[bcname], bc_value={"Back": (0.3, -0.2, 1.0)})
+    st = _random_state((17, 15, 13), 11)
+    s, o = _pair(orc, p, g, st)
+    got = s.get_state()
+    for k, a in zip(FIELDS, got):
+        np.testing.assert_array_equal(a, o.get(k), err_msg=k)
+
+
+@pytest.mark.parametrize("bcname", list(BCS))
+@pytest.mark.parametrize("sweeps", [0, 7])
+def test_one_step_forced_sweeps(orc, bcname, sweeps):
+    """A full loop body with a fixed sweep count (itmax = sweeps, zeta = 0)."""
+    n = (13, 11, 9)
+    g = orc.gridder_unequal(*n, 1.0, 1.3, 1.7,
+                            (12.5, 0.65, 0.6, 16, 4, 6, 4, 6, 1.0, 0.1, 0.3, 0.2, 0.5))
+    p = make_params(*n, Re=100.0, dt=f4(1e-3), zeta=0.0, itmax=sweeps, bc=BCS[bcname],
+                    bc_value={"Back": (0.3, -0.2, 1.0)})
+    s, o = _pair(orc, p, g, _random_state((17, 15, 13), 5))
+    info, rc = s.step(1)
+    oi = o.step(1, forced=[sweeps])
+    assert info[0].sor_iters == sweeps
+    assert rc == (abi.NTCFD_NOT_CONVERGED if sweeps > 0 else abi.NTCFD_NOT_CONVERGED)
+    _compare(s, o, 1e-12)
+
+
+@pytest.mark.parametrize("mode", [SMAG_REF_ALIASED, SMAG_STAGGERED])
+def test_les_step_parity(orc, mode):
+    n = (12, 10, 14)
+    g = orc.gridder_equal(*n, 1.0, 1.0, 1.0)
+    p = make_params(*n, Re=1000.0, dt=f4(1e-3), zeta=0.0, itmax=5, LES=1, Cs=f4(0.1),
+                    smag_mode=mode, bc=BCS["cavity"])
+    s, o = _pair(orc, p, g, _random_state((16, 14, 18), 9))
+    s.step(2)
+    o.step(2, forced=[5, 5])
+    _compare(s, o, 1e-12)
+
+
+def test_c1_cavity_parity():
+    pass
+
+
+@pytest.fixture(scope="module")
+def c1_runs(orc):
+    """C1: 40^3 cavity, Re=100, dt=1e-3, lid u=1, zeta=1e-4, 200 steps."""
+    from ntustcfdlab_b200 import cases
+    c = cases.c1()
+    s = _solver(c.params, c.grid)
+    s.boundary_conditions()
+    info, rc = s.step(c.steps)
+    gpu_sweeps = [i.sor_iters for i in info]
+    o_rb = orc.Oracle(c.params, c.grid)
+    o_rb.initial_conditions(); o_rb.boundary_conditions()
+    o_info = o_rb.step(c.steps)
+    return dict(case=c, s=s, info=info, rc=rc, gpu_sweeps=gpu_sweeps, o_rb=o_rb, o_info=o_info)
+
+
+def test_c1_sweep_counts_match_oracle(c1_runs):
+    g = c1_runs["gpu_sweeps"]
+    o = [i.sor_iters for i in c1_runs["o_info"]]
+    assert c1_runs["rc"] == 0
+    assert all(i.converged for i in c1_runs["info"])
+    assert g == o
+
+
+def test_c1_fields_match_oracle_redblack(c1_runs):
+    out = _compare(c1_runs["s"], c1_runs["o_rb"], 1e-12)
+    print("C1 GPU vs oracle red-black rel-L2:", out)
+
+
+def test_c1_outputs_and_forces(c1_runs):
+    s, o = c1_runs["s"], c1_runs["o_rb"]
+    pre, uc, vc, wc = s.get_output()
+    for k, a in (("pre", pre), ("uc", uc), ("vc", vc), ("wc", wc)):
+        assert rel_l2(a, o.get(k)) <= 1e-12, k
+    assert all(i.cDrag == 0.0 and i.cLift == 0.0 for i in c1_runs["info"])
+    assert s.time == pytest.approx(c1_runs["o_rb"].time, rel=0, abs=0)
+
+
+def test_c1_against_reference_ordering(orc, c1_runs):
+    """GPU red-black vs the reference's lexicographic ordering, both stopping
+    at zeta = 1e-4: the orderings reach different iterates of the same solve,
+    so the agreement is bounded by the stop rule, not by round-off."""
+    c = c1_runs["case"]
+    o_lex = orc.Oracle(params_copy(c.params, sor_order=SOR_LEX), c.grid)
+    o_lex.initial_conditions(); o_lex.boundary_conditions()
+    o_lex.step(c.steps)
+    got = dict(zip(FIELDS, c1_runs["s"].get_state()))
+    errs = {k: rel_l2(interior(got[k]), interior(o_lex.get(k))) for k in FIELDS}
+    print("C1 GPU red-black vs oracle lexicographic rel-L2:", errs)
+    for k in ("u", "v", "w"):
+        assert errs[k] < 2e-3, (k, errs[k])
+    assert errs["p"] < 2e-2
+
+
+def test_mixed_precision_matches_fp64():
+    from ntustcfdlab_b200 import cases
+    c64 = cases.cavity(48, 1000.0, 5e-4, 40, precision=FP64)
+    c32 = cases.cavity(48, 1000.0, 5e-4, 40, precision=MIXED)
+    res = []
+    for c in (c64, c32):
+        s = _solver(c.params, c.grid)
+        s.boundary_conditions()
+        info, rc = s.step(c.steps)
+        assert rc == 0
+        res.append((s.get_state(), [i.sor_iters for i in info]))
+    errs = {k: rel_l2(interior(a), interior(b)) for k, a, b in zip(FIELDS, res[1][0], res[0][0])}
+    print("mixed vs FP64 rel-L2:", errs, "sweeps", sum(res[0][1]), sum(res[1][1]))
+    for k in FIELDS:
+        assert errs[k] < 1e-5, (k, errs[k])
+
+
+def test_cylinder_mask_exact(orc):
+    n = (4, 48, 40)
+    g = orc.gridder_equal(*n, 1.0, 6.0, 5.0)
+    p = make_params(*n, Re=100.0, dt=1e-3)
+    s = _solver(p, g)
+    s.build_mask_cylinder(2.0, 3.0, 0.5)
+    o = orc.Oracle(p, g)
+    o.cylinder(2.0, 3.0, 0.5)
+    np.testing.assert_array_equal(s.get_mask(), o.get("ETA"))
+
+
+def test_naca_mask_exact(orc):
+    from ntustcfdlab_b200.solver import naca4_polygon
+    n = (3, 96, 120)
+    band = (12.5, f4(3.948), f4(3.95), 16, 30, 45, 40, 55, 1.0, f4(0.3), f4(0.6), f4(1.1), 2.0)
+    g = orc.gridder_unequal(*n, 1.0, 8.0, 10.0, band)
+    p = make_params(*n, Re=100.0, dt=1e-3)
+    z, y = naca4_polygon(0.12, 256)
+    s = _solver(p, g)
+    ties = s.build_mask_polygon(z, y, 5.0, 4.0, 4.0)
+    o = orc.Oracle(p, g)
+    oties = o.raycasting(z, y, 5.0, 4.0, 4.0)
+    assert ties == 0 and oties == 0
+    eta = s.get_mask()
+    np.testing.assert_array_equal(eta, o.get("ETA"))
+    assert 0.0 < eta.max() <= 1.0 and eta.sum() > 0
+
+
+def test_cylinder_forces_parity(orc):
+    """Direct forcing on a cylinder in a channel: forces and fields."""
+    n = (4, 32, 48)
+    g = orc.gridder_equal(*n, 0.5, 4.0, 6.0)
+    bc = {"West": ("periodic",) * 3, "East": ("periodic",) * 3,
+          "South": ("Neumann",) * 3, "North": ("Neumann",) * 3,
+          "Back": ("Dirichlet", "Dirichlet", "Dirichlet"), "Front": ("Neumann",) * 3}
+    p = make_params(*n, Re=100.0, dt=f4(1e-3), zeta=0.0, itmax=6, bc=bc,
+                    bc_value={"Back": (0.0, 0.0, 1.0)}, lx=0.5)
+    s, o = _pair(orc, p, g)
+    s.build_mask_cylinder(2.0, 2.0, 0.5)
+    o.cylinder(2.0, 2.0, 0.5)
+    info, _ = s.step(3)
+    oi = o.step(3, forced=[6, 6, 6])
+    for a, b in zip(info, oi):
+        assert a.cDrag == pytest.approx(b.cDrag, rel=1e-10, abs=1e-14)
+        assert a.cLift == pytest.approx(b.cLift, rel=1e-9, abs=1e-12)
+    assert abs(info[-1].cDrag) > 0
+    _compare(s, o, 1e-12)
+
+
+def test_not_converged_is_a_warning():
+    from ntustcfdlab_b200 import cases
+    c = cases.cavity(16, 100.0, 1e-3, 2)
+    p = params_copy(c.params, itmax=2, zeta=0.0)
+    s = _solver(p, c.grid)
+    s.boundary_conditions()
+    info, rc = s.step(2)
+    assert rc == abi.NTCFD_NOT_CONVERGED
+    assert [i.sor_iters for i in info] == [2, 2] and not any(i.converged for i in info)
+
+
+def test_nonfinite_state_is_reported():
+    from ntustcfdlab_b200 import cases
+    from ntustcfdlab_b200.solver import NtcfdError
+    c = cases.cavity(16, 100.0, 1e-3, 1)
+    s = _solver(c.params, c.grid)
+    st = [np.zeros((20, 20, 20), order="F") for _ in range(4)]
+    st[0][8, 8, 8] = np.nan
+    s.set_state(*st)
+    with pytest.raises(NtcfdError) as e:
+        s.step(1)
+    assert e.value.code == abi.NTCFD_ENONFINITE
