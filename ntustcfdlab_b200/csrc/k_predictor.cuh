@@ -162,7 +162,8 @@ __device__ __forceinline__ double phi_read(const Geom& g, const double* f, int i
     const long long t = off / ax;
     const int b = (int)(t % ay);
     const int cc = (int)(t / ay);
-    return __ldg(f + nat(g, a - 2, b - 2, cc - 2));
+    // storage element `off` counted from u(-1,-1,-1): Fortran index = position - 1
+    return __ldg(f + nat(g, a - 1, b - 1, cc - 1));
 }
 
 __device__ __forceinline__ void grad_gauss(const Geom& g, const double* f, bool al, int i, int j, int k,

@@ -308,7 +308,7 @@ int validate(const ntcfd_params* p, std::string* why) {
             return NTCFD_EINVAL;
         }
     }
-    for (int q = 0; q < 6; ++q)
+    for (size_t q = 0; q < sizeof p->reserved / sizeof p->reserved[0]; ++q)
         if (p->reserved[q] != 0) return bad("reserved fields must be zero");
     return 0;
 }
