@@ -42,7 +42,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     os.makedirs(LIB_DIR, exist_ok=True)
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared",
            "-Xcompiler", "-fPIC,-ffp-contract=off", "-ccbin", "g++",
-           "-o", OUT + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart"]
+           "-cudart", "static", "-o", OUT + ".tmp", *[os.path.join(CSRC, s) for s in SOURCES]]
     if extra:
         cmd[1:1] = extra
     if verbose:
