@@ -130,6 +130,30 @@ int ntcfd_get_mask(ntcfd_ctx* ctx, double* eta);
  * the reference resolves by moving the grid (airfoil.f90:700-702). */
 int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
                              double aoa_deg, double zc, double yc, int* ties_out);
+/* Same result as ntcfd_build_mask_polygon, for callers that must not
+ * allocate device memory after set-up.  No counterpart in the reference.
+ *
+ * ntcfd_build_mask_polygon allocates and frees device scratch (the moved
+ * polygon, the cut-cell list, a tie counter) on every call.  A driver that
+ * rebuilds the mask inside its time loop -- a dynamic angle of attack re-runs
+ * the ray casting every step -- cannot afford that: cudaFree waits for all
+ * work on the device, so each step would stall, and a caller whose device
+ * memory is already handed out to its own allocator may find cudaMalloc
+ * failing mid-run.  This variant keeps that scratch in one fixed array that
+ * the library reserves on every device that loads it (2.25 MiB, held
+ * until the process exits) and calls no cudaMalloc, cudaFree or other
+ * allocating routine; ETA goes to the context's existing storage.
+ *
+ * Limits: npts <= 16384 polygon points and ny*nz <= 262144 cells in the
+ * (k,j) plane; larger inputs return NTCFD_EINVAL before any device work.
+ * The first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls on a
+ * device share the array: the tie counter and the cut-cell flags are cleared
+ * by each call, and two calls that overlap on the GPU (from two host threads
+ * or two contexts on one device) race on it. */
+int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az, const double* ay,
+                                     int npts, double aoa_deg, double zc, double yc,
+                                     int* ties_out);
 /* DFIB_Cylinder (DFIB.f90:74-145): cylinder along x, centre (zc, yc), radius r,
  * 50x50 sub-cells within half a cell diagonal of the surface, real*4 arithmetic. */
 int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r);

@@ -133,6 +133,9 @@ SIGNATURES = {
     "ntcfd_build_mask_polygon": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int,
                                                 ctypes.c_double, ctypes.c_double,
                                                 ctypes.c_double, _IP]),
+    "ntcfd_build_mask_polygon_noalloc": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int,
+                                                        ctypes.c_double, ctypes.c_double,
+                                                        ctypes.c_double, _IP]),
     "ntcfd_build_mask_cylinder": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double,
                                                  ctypes.c_double, ctypes.c_double]),
     "ntcfd_set_state": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),

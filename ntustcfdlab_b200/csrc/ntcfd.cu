@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <utility>
@@ -873,4 +874,123 @@ int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* 
     return 0;
 }
 
+// ------------------------------------------- ray casting without allocation
 }  // extern "C"
+
+// Scratch of ntcfd_build_mask_polygon_noalloc: one fixed device array per
+// device that loads the library.  Layout: az[kNaPoly], ay[kNaPoly] (double),
+// points[kNaCells], list[kNaCells] (int), the tie counter (int).
+namespace {
+constexpr int kNaPoly = 16384;
+constexpr int kNaCells = 1 << 18;
+constexpr size_t kNaPointsOff = 2 * sizeof(double) * (size_t)kNaPoly;
+constexpr size_t kNaListOff = kNaPointsOff + sizeof(int) * (size_t)kNaCells;
+constexpr size_t kNaTiesOff = kNaListOff + sizeof(int) * (size_t)kNaCells;
+constexpr size_t kNaBytes = kNaTiesOff + 256;   // 2.25 MiB + 256 B
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_mask_scratch[kNaBytes];
+
+namespace {
+std::mutex g_na_mu;
+void* g_na_addr[256] = {};
+
+// Device address of g_mask_scratch on the current device (the context's),
+// looked up once per device: in host code the symbol is only a stand-in.
+int noalloc_scratch(ntcfd_ctx* ctx, unsigned char** out) {
+    const int dev = ctx->prm.device;
+    if (dev < 0 || dev >= 256) return fail(ctx, NTCFD_EINVAL, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_addr[dev]) {
+        void* a = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&a, g_mask_scratch);
+        if (e != cudaSuccess || !a)
+            return fail(ctx, NTCFD_ECUDA, "cudaGetSymbolAddress(g_mask_scratch) failed: %s",
+                        cudaGetErrorString(e));
+        g_na_addr[dev] = a;
+    }
+    *out = (unsigned char*)g_na_addr[dev];
+    return 0;
+}
+}  // namespace
+
+extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az_in, const double* ay_in,
+                                                int npts, double aoa, double zc, double yc, int* ties_out) {
+    DEV();
+    if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
+    if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    const Geom& g = ctx->g;
+    const size_t cells = (size_t)g.ny * g.nz;
+    if (npts > kNaPoly)
+        return fail(ctx, NTCFD_EINVAL, "polygon has %d points; the allocation-free variant takes at most %d",
+                    npts, kNaPoly);
+    if (cells > (size_t)kNaCells)
+        return fail(ctx, NTCFD_EINVAL, "ny*nz = %zu cells; the allocation-free variant takes at most %d",
+                    cells, kNaCells);
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(ctx, &base)) return rc;
+    double* daz = reinterpret_cast<double*>(base);
+    double* day = daz + kNaPoly;
+    int* points = reinterpret_cast<int*>(base + kNaPointsOff);
+    int* list = reinterpret_cast<int*>(base + kNaListOff);
+    int* ties = reinterpret_cast<int*>(base + kNaTiesOff);
+    // polygon transform of airfoil.f90:597-611 (host)
+    std::vector<double> az(az_in, az_in + npts), ay(ay_in, ay_in + npts);
+    const double PI = 4.0 * std::atan(1.0);
+    for (int i = 0; i < npts; ++i) {
+        az[i] = az[i] - 0.25;
+        az[i] = std::cos((-aoa) * PI / 180) * az[i] - std::sin((-aoa) * PI / 180) * ay[i];
+        ay[i] = std::sin((-aoa) * PI / 180) * az[i] + std::cos((-aoa) * PI / 180) * ay[i];
+        az[i] = az[i] + zc;
+        ay[i] = ay[i] + yc;
+        az[i] = az[i] + 0.25;
+    }
+    std::vector<double> Y(g.ny + 5), Z(g.nz + 5);
+    CK(cudaMemcpyAsync(Y.data(), ctx->coordbuf, (g.ny + 5) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(Z.data(), ctx->coordbuf + (g.ny + 5) + 4, (g.nz + 5) * sizeof(double),
+                       cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    double miny = ay[0], maxy = ay[0], minz = az[0], maxz = az[0];
+    for (int i = 1; i < npts; ++i) {
+        miny = std::min(miny, ay[i]); maxy = std::max(maxy, ay[i]);
+        minz = std::min(minz, az[i]); maxz = std::max(maxz, az[i]);
+    }
+    int A = 0, B = 0, C = 0, E = 0;   // airfoil.f90:615-654
+    for (int j = 1; j <= g.ny; ++j) if (Y[j + 1] > miny) { A = j - 1; break; }
+    for (int j = 1; j <= g.ny; ++j) if (Y[j + 1] > maxy) { B = j; break; }
+    for (int k = 1; k <= g.nz; ++k) if (Z[k + 1] > minz) { C = k - 1; break; }
+    for (int k = 1; k <= g.nz; ++k) if (Z[k + 1] > maxz) { E = k; break; }
+    // the array keeps the previous call's contents: clear the flags and the counter
+    CK(cudaMemsetAsync(points, 0, sizeof(int) * cells, ctx->stream));
+    CK(cudaMemsetAsync(ties, 0, sizeof(int), ctx->stream));
+    CK(cudaMemcpyAsync(daz, az.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(day, ay.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
+    double* eta1 = ctx->outbuf;
+    k_ray_main<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+        g.ny, g.nz, ctx->coordY, ctx->coordZ, daz, day, npts, eta1, ties);
+    k_ray_points<<<(npts + 127) / 128, 128, 0, ctx->stream>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, daz,
+                                                                day, npts, A, B, C, E, points);
+    std::vector<int> hp(cells);
+    CK(cudaMemcpyAsync(hp.data(), points, sizeof(int) * cells, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<int> hl;
+    for (size_t q = 0; q < cells; ++q)
+        if (hp[q]) hl.push_back((int)q);
+    if (!hl.empty()) {
+        CK(cudaMemcpyAsync(list, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice, ctx->stream));
+        k_ray_sub<256><<<(unsigned)hl.size(), 256, 0, ctx->stream>>>(g.nz, ctx->coordY, ctx->coordZ, daz,
+                                                                    day, npts, list, eta1, ties);
+    }
+    const dim3 b3(32, 4, 2);
+    k_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), b3, 0, ctx->stream>>>(
+        g, eta1, ctx->eta);
+    int hties = 0;
+    CK(cudaMemcpyAsync(&hties, ties, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ties_out) *ties_out = hties;
+    if (hties)
+        return fail(ctx, NTCFD_EINVAL,
+                    "%d exact vertex/grid ties: the reference resolves them by moving the grid", hties);
+    return 0;
+}
