@@ -53,6 +53,14 @@ enum { NTCFD_FP64 = 0, NTCFD_MIXED = 1 };
 enum { NTCFD_QUICK_CENTRE = 0 };                       /* discretisation_QUICK_centre.f90 */
 enum { NTCFD_SMAG_REF_ALIASED = 0, NTCFD_SMAG_STAGGERED = 1 };
 enum { NTCFD_SOR_REDBLACK = 0, NTCFD_SOR_LEX = 1 };    /* LEX: oracle only */
+/* How the sweeps of one correction cycle run on the device:
+ * STREAMING -- two kernels per sweep (one per colour) reading e from
+ *              global memory, the loop driven by CUDA-graph conditional nodes;
+ * RESIDENT  -- one persistent cooperative kernel per cycle with e kept in
+ *              shared memory (only when the grid's e fits on the chip);
+ * AUTO      -- RESIDENT when it fits, else STREAMING.  Both run the same
+ *              red-black iteration and stop rule. */
+enum { NTCFD_SOR_AUTO = 0, NTCFD_SOR_STREAMING = 1, NTCFD_SOR_RESIDENT = 2 };
 
 typedef struct ntcfd_params {
     int nx, ny, nz;          /* interior cells (variables_module.f90:13-17) */
@@ -75,7 +83,8 @@ typedef struct ntcfd_params {
     int mixed_cycle;         /* MIXED: max FP32 sweeps per defect-correction cycle (0 = itmax) */
     int diag_divergence;     /* 1: report max|div u^{n+1}| in ntcfd_step_info.div_max */
     int device;              /* CUDA device ordinal that holds the grid */
-    int reserved[5];         /* must be zero */
+    int sor_path;            /* NTCFD_SOR_AUTO, NTCFD_SOR_STREAMING or NTCFD_SOR_RESIDENT */
+    int reserved[4];         /* must be zero */
 } ntcfd_params;
 
 typedef struct ntcfd_step_info {
@@ -86,6 +95,8 @@ typedef struct ntcfd_step_info {
     double div_max;          /* max |div u^{n+1}| * V (FP64) when diag_divergence = 1 */
     int dc_cycles;           /* defect-correction cycles used */
     int launches;            /* device kernels launched for this step */
+    int sor_path;            /* NTCFD_SOR_STREAMING or NTCFD_SOR_RESIDENT: the path that ran */
+    int pad;
 } ntcfd_step_info;
 
 /* Average device time of single kernels of the step, for the roofline. */
@@ -96,7 +107,8 @@ typedef struct ntcfd_kernel_times {
     float sweep_ms;          /* one half-sweep (one colour) */
     float project_ms;        /* K4, measured on a copy of the velocity */
     float bc_ms;             /* the three K6 launches together */
-    float reserved[2];
+    float resident_ms;       /* one resident-SOR launch running resident_sweeps sweeps (0 if unused) */
+    float resident_sweeps;
 } ntcfd_kernel_times;
 
 typedef struct ntcfd_ctx ntcfd_ctx;

@@ -29,6 +29,7 @@ FP64, MIXED = 0, 1
 QUICK_CENTRE = 0
 SMAG_REF_ALIASED, SMAG_STAGGERED = 0, 1
 SOR_REDBLACK, SOR_LEX = 0, 1
+SOR_AUTO, SOR_STREAMING, SOR_RESIDENT = 0, 1, 2
 
 # boundary-condition strings of variables_module.f90:110-132
 BC_NAMES = {"no-slip": BC_NOSLIP, "Neumann": BC_NEUMANN, "Dirichlet": BC_DIRICHLET,
@@ -53,7 +54,8 @@ class NtcfdParams(ctypes.Structure):
         ("mixed_cycle", ctypes.c_int),
         ("diag_divergence", ctypes.c_int),
         ("device", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("sor_path", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -64,12 +66,14 @@ class NtcfdStepInfo(ctypes.Structure):
         ("cDrag", ctypes.c_double), ("cLift", ctypes.c_double),
         ("div_max", ctypes.c_double),
         ("dc_cycles", ctypes.c_int), ("launches", ctypes.c_int),
+        ("sor_path", ctypes.c_int), ("pad", ctypes.c_int),
     ]
 
 
 class NtcfdKernelTimes(ctypes.Structure):
     _fields_ = [(n, ctypes.c_float) for n in ("predictor_ms", "rhs_ms", "defect_ms", "sweep_ms",
-                                              "project_ms", "bc_ms", "r0", "r1")]
+                                              "project_ms", "bc_ms", "resident_ms",
+                                              "resident_sweeps")]
 
 
 def f4(x: float) -> float:
@@ -82,7 +86,7 @@ def make_params(nx, ny, nz, *, Re, dt, omega=1.5, zeta=f4(1e-4), itmax=3000, LES
                 Cs=f4(0.18), precision=FP64, sor_order=SOR_REDBLACK,
                 smag_mode=SMAG_REF_ALIASED, check_every=1, bc=None, bc_value=None,
                 u_solid=(0.0, 0.0, 0.0), lx=1.0, mixed_cycle=0,
-                diag_divergence=0, device=0) -> NtcfdParams:
+                diag_divergence=0, device=0, sor_path=SOR_AUTO) -> NtcfdParams:
     """Builds an ``ntcfd_params``.  ``bc`` maps wall name -> (u, v, w) kind
     strings; missing walls are no-slip, as in variables_module.f90:110-132."""
     p = NtcfdParams()
@@ -105,6 +109,7 @@ def make_params(nx, ny, nz, *, Re, dt, omega=1.5, zeta=f4(1e-4), itmax=3000, LES
     p.mixed_cycle = mixed_cycle
     p.diag_divergence = diag_divergence
     p.device = device
+    p.sor_path = sor_path
     return p
 
 

@@ -24,9 +24,13 @@ struct SorCoef {
     const Tc *cE, *cW, *cN, *cS, *cF, *cB;
 };
 
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+
+// 1 / sum of the six coefficients (correctly rounded reciprocal)
 template <class Tc>
 __device__ __forceinline__ Tc rdiag_of(const SorCoef<Tc>& s, int i, int j, int k) {
-    return Tc(1) / (((s.cE[i] + s.cW[i]) + (s.cN[j] + s.cS[j])) + (s.cF[k] + s.cB[k]));
+    return rcp_rn(((s.cE[i] + s.cW[i]) + (s.cN[j] + s.cS[j])) + (s.cF[k] + s.cB[k]));
 }
 
 // K3a -- b' on the interior from the predicted velocity (GS.f90:39-41).
@@ -51,18 +55,23 @@ __global__ void __launch_bounds__(256) k_rhs(Geom g, SorCoef<double> sc, const d
 // Defect d = rdiag*sum c p0_nb - b' - p0 in double, stored per colour in
 // Tc; e reset to 0.  Inside the step graph (in_graph = 1) it also arms the
 // inner loop's condition.
+// For the resident path (ring != null) it also clears the ring of sweep
+// maxima and the grid barrier the next kernel uses.
 template <class Tc>
 __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, const double* p,
                                                 const double* b, Tc* dR, Tc* dB, Tc* eR, Tc* eB,
                                                 Ctl* ctl, cudaGraphConditionalHandle inner,
-                                                int in_graph) {
+                                                int in_graph, unsigned long long* ring,
+                                                unsigned int* bar) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (in_graph && blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
+    if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
         threadIdx.y == 0 && threadIdx.z == 0) {
         ctl->inner = 0;
-        cudaGraphSetConditional(inner, 1u);
+        if (in_graph) cudaGraphSetConditional(inner, 1u);
+        if (ring) { ring[0] = 0ULL; ring[1] = 0ULL; ring[2] = 0ULL; }
+        if (bar) { bar[0] = 0u; bar[2] = 0u; }   // GridBar count and err
     }
     if (i > g.nx || j > g.ny || k > g.nz) return;
     const long long c = nat(g, i, j, k);
@@ -74,53 +83,105 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
     else { dB[q] = (Tc)d; eB[q] = Tc(0); }
 }
 
-// One half-sweep over colour `colour` (0 = red, (i+j+k) even).  Thread t of
-// row (j,k) owns the cell i = 2t + 2 - r, m = t + 2 - r, r = ((j+k)^colour)&1.
-// `sub` is the index of this sweep inside the loop body; the sweep is skipped
-// once the sweep budget (itmax, cycle length) is used up.
-template <class Tc, int NT>
-__global__ void __launch_bounds__(NT) k_sweep(Geom g, SorCoef<Tc> sc, Tc* eOwn, const Tc* eOth,
-                                              const Tc* dOwn, int colour, double omega, Ctl* ctl,
-                                              int sub, int itmax, int cycle_len,
-                                              unsigned long long* slots) {
-    const int ik = ctl->ik, inner = ctl->inner;
-    if (ik + sub >= itmax || inner + sub >= cycle_len) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+// rd = 1 / sum of the six coefficients of every interior cell, per colour,
+// in the sweeps' precision; it depends on the grid only and is made once.
+template <class Tc>
+__global__ void k_make_rd(Geom g, SorCoef<Tc> sc, Tc* rdR, Tc* rdB) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    double ch = 0.0;
-    if (j <= g.ny && k <= g.nz) {
-        const int r = ((j + k) ^ colour) & 1;
-        const int i = 2 * t + 2 - r;
-        if (i >= 1 && i <= g.nx) {
-            const int m = t + 2 - r;
-            const long long q = spl(g, m, j, k);
-            const Tc s = sc.cE[i] * eOth[q + r] + sc.cW[i] * eOth[q - 1 + r] +
-                         sc.cN[j] * eOth[q + g.mxp] + sc.cS[j] * eOth[q - g.mxp] +
-                         sc.cF[k] * eOth[q + g.mz] + sc.cB[k] * eOth[q - g.mz];
-            const Tc eNew = rdiag_of(sc, i, j, k) * s + dOwn[q];
-            const Tc e0 = eOwn[q];
-            const Tc diff = eNew - e0;
-            eOwn[q] = e0 + (Tc)omega * diff;
-            ch = (double)fabs(diff);
-        }
-    }
-    block_max_atomic<NT>(ch, &slots[sub]);
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long q = spl(g, (i + 2) >> 1, j, k);
+    const Tc rd = rdiag_of(sc, i, j, k);
+    if (((i + j + k) & 1) == 0) rdR[q] = rd;
+    else rdB[q] = rd;
 }
 
-// Loop control after a group of `csweeps` sweeps (one WHILE body).
-// Implements `do while (pChangeMax_ > zeta .and. ik < itmax)` (GS.f90:11)
-// on the change of the last sweep that ran; a cycle of the mixed path also
-// ends after cycle_len sweeps.
+// One half-sweep over colour `colour` (0 = red, (i+j+k) even).  Thread t of
+// row (j,k) owns the cell i = 2t + 2 - r, m = t + 2 - r, r = ((j+k)^colour)&1,
+// for KPT consecutive planes k; all loads of the KPT cells are issued before
+// any arithmetic so that a warp keeps 9*KPT loads in flight.  Offsets are
+// 32-bit (a grid holds fewer than 2^31 cells per colour array).  With
+// guard = 1 (several sweeps per loop body) the sweep is skipped once the
+// sweep budget (itmax, cycle length) is used up.  The block's max |change|
+// goes to slot sub*kSpread + (block index mod kSpread).
+template <class Tc, int NT, int KPT>
+__global__ void __launch_bounds__(NT) k_sweep(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
+                                              const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
+                                              const Tc* __restrict__ rdOwn, int colour, double omega,
+                                              const Ctl* ctl, int sub, int itmax, int cycle_len,
+                                              int guard, unsigned long long* slots) {
+    if (guard) {
+        const int ik = ctl->ik, inner = ctl->inner;
+        if (ik + sub >= itmax || inner + sub >= cycle_len) return;
+    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k0 = blockIdx.z * KPT + 1;
+    const Tc om = (Tc)omega;
+    using B = decltype(abs_bits(Tc(0)));
+    const bool jok = j <= g.ny;
+    const int jj = jok ? j : g.ny;
+    const int ys = g.mxp, zs = (int)g.mz;
+    const int rowj = ys * (jj + 1);
+    int q[KPT];
+    bool ok[KPT];
+    Tc nE[KPT], nW[KPT], nN[KPT], nS[KPT], nF[KPT], nB[KPT], dd[KPT], e0[KPT], rd[KPT];
+#pragma unroll
+    for (int kk = 0; kk < KPT; ++kk) {
+        const int k = min(k0 + kk, g.nz);
+        const int r = ((jj + k) ^ colour) & 1;
+        const int i = 2 * t + 2 - r;
+        ok[kk] = jok && (k0 + kk <= g.nz) && i <= g.nx;
+        // an inactive lane reads a valid interior cell and discards it
+        const int rr = ok[kk] ? r : 1;
+        const int qq = (ok[kk] ? t + 2 - r : 1) + rowj + zs * (k + 1);
+        q[kk] = qq;
+        nE[kk] = eOth[qq + rr];
+        nW[kk] = eOth[qq - 1 + rr];
+        nN[kk] = eOth[qq + ys];
+        nS[kk] = eOth[qq - ys];
+        nF[kk] = eOth[qq + zs];
+        nB[kk] = eOth[qq - zs];
+        dd[kk] = dOwn[qq];
+        e0[kk] = eOwn[qq];
+        rd[kk] = rdOwn[qq];
+    }
+    const Tc cN = sc.cN[jj], cS = sc.cS[jj];
+    B ch = B(0);   // max |change| as an order-preserving pattern (NaN stays on top)
+#pragma unroll
+    for (int kk = 0; kk < KPT; ++kk) {
+        if (!ok[kk]) continue;
+        const int k = k0 + kk;
+        const int i = 2 * t + 2 - (((j + k) ^ colour) & 1);
+        const Tc s = sc.cE[i] * nE[kk] + sc.cW[i] * nW[kk] + cN * nN[kk] + cS * nS[kk] +
+                     sc.cF[k] * nF[kk] + sc.cB[k] * nB[kk];
+        const Tc diff = (rd[kk] * s + dd[kk]) - e0[kk];
+        eOwn[q[kk]] = e0[kk] + om * diff;
+        const B db = abs_bits(diff);
+        ch = db > ch ? db : ch;
+    }
+    const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    block_max_bits<NT>(ch, &slots[sub * kSpread + (blin & (kSpread - 1))]);
+}
+
+// One warp: the max over the kSpread slots of that sweep is its max|change|.
 __global__ void k_sor_check(Ctl* ctl, unsigned long long* slots, int csweeps, int itmax,
                             int cycle_len, double zeta, cudaGraphConditionalHandle inner) {
+    const int lane = threadIdx.x;
     const int ik = ctl->ik, in = ctl->inner;
     int ran = csweeps;
     if (itmax - ik < ran) ran = itmax - ik;
     if (cycle_len - in < ran) ran = cycle_len - in;
     if (ran < 0) ran = 0;
-    unsigned long long bits = ran > 0 ? slots[ran - 1] : 0ULL;
-    for (int s = 0; s < csweeps; ++s) slots[s] = 0ULL;
+    unsigned long long bits = ran > 0 ? slots[(ran - 1) * kSpread + lane] : 0ULL;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t2 = __shfl_xor_sync(0xffffffffu, bits, o);
+        bits = t2 > bits ? t2 : bits;
+    }
+    for (int s = 0; s < csweeps; ++s) slots[s * kSpread + lane] = 0ULL;
+    if (lane != 0) return;
     const double change = __longlong_as_double((long long)bits);
     ctl->ik = ik + ran;
     ctl->inner = in + ran;
@@ -152,6 +213,7 @@ __global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle oute
     ctl->inner = 0;
     ctl->cycles = 0;
     ctl->bodies = 0;
+    ctl->timeout = 0;
     ctl->converged = 0;
     ctl->nonfinite = 0;
     ctl->last_change = 0.0;
@@ -162,7 +224,7 @@ __global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle oute
 // stopped on its cycle length.
 __global__ void k_outer_check(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer) {
     ctl->cycles += 1;
-    const bool more = !ctl->converged && !ctl->nonfinite && ctl->ik < itmax;
+    const bool more = !ctl->converged && !ctl->nonfinite && !ctl->timeout && ctl->ik < itmax;
     cudaGraphSetConditional(outer, more ? 1u : 0u);
 }
 

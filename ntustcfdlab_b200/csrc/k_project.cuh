@@ -412,15 +412,16 @@ __global__ void __launch_bounds__(NT) k_divmax(Geom g, const double* u, const do
         d = fabs((u[c] - u[c - 1]) * g.iDy[j] * g.iDz[k] + (v[c] - v[c - g.px]) * g.iDx[i] * g.iDz[k] +
                  (w[c] - w[c - g.pz]) * g.iDx[i] * g.iDy[j]);
     }
-    block_max_atomic<NT>(d, slot);
+    block_max_atomic<NT>(d, slot);  // one slot: the diagnostic runs once per step
 }
 
 // Records the step; `fixed` kernels per step, 3 per correction cycle and
 // 2*csweeps + 1 per inner loop body.
 __global__ void k_step_end(Ctl* ctl, StepRec* rec, unsigned long long* divslot, int diag,
-                           int fixed, int csweeps) {
+                           int fixed, int per_body) {
     const int s = ctl->step;
-    rec[s].launches = fixed + 3 * ctl->cycles + ctl->bodies * (2 * csweeps + 1);
+    rec[s].launches = fixed + 3 * ctl->cycles + ctl->bodies * per_body;
+    rec[s].timeout = ctl->timeout;
     rec[s].sor_iters = ctl->ik;
     rec[s].converged = ctl->converged;
     rec[s].last_change = ctl->last_change;

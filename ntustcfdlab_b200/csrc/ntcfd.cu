@@ -24,6 +24,7 @@
 #include "k_predictor.cuh"
 #include "k_pressure.cuh"
 #include "k_project.cuh"
+#include "k_resident.cuh"
 #include "ntcfd_common.cuh"
 
 using namespace ntcfd;
@@ -33,6 +34,10 @@ namespace {
 constexpr int kProjKc = 8;      // planes per column chunk in K4
 constexpr int kSweepBx = 64;    // threads per row in a half-sweep
 constexpr int kSweepBy = 4;
+constexpr int kSweepKpt = 4;     // planes per thread in a half-sweep
+constexpr int kResNT = 512;      // threads per CTA of the resident SOR kernel
+const double kZeroZeta = 0.0;
+const int kOne = 1;
 
 struct DevTabs {
     // one allocation per precision; every table has n+5 entries (index -2..n+2)
@@ -51,6 +56,7 @@ struct ntcfd_ctx {
     double *us = nullptr, *vs = nullptr, *ws = nullptr, *b = nullptr;
     double *eta = nullptr, *nut = nullptr;
     void *eR = nullptr, *eB = nullptr, *dR = nullptr, *dB = nullptr;
+    void *rdR = nullptr, *rdB = nullptr;   // 1/diag per colour (sweep precision)
     double* tabd = nullptr;   // double tables
     float* tabf = nullptr;    // float tables
     Tabs<double> tpd{};
@@ -68,6 +74,14 @@ struct ntcfd_ctx {
     int rec_cap = 0;
     unsigned long long* slots = nullptr;   // per-sweep max |change| bits
     unsigned long long* divslot = nullptr;
+    GridBar* bar = nullptr;                 // grid barrier of the resident SOR kernel
+    unsigned long long* ring = nullptr;     // its per-sweep max |change| ring
+    Brick brick{};
+    bool resident = false;                  // the graph uses the resident SOR kernel
+    size_t res_smem = 0;
+    int res_grid = 0;
+    int sm_count = 0;
+    size_t smem_optin = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -143,6 +157,29 @@ cudaError_t add_kernel(cudaGraphNode_t* out, cudaGraph_t g, const std::vector<cu
     return cudaGraphAddKernelNode(out, g, deps.data(), deps.size(), &kp);
 }
 
+// A kernel node with dynamic shared memory, optionally cooperative (all CTAs
+// co-resident, required by the grid barrier of the resident SOR kernel).
+template <class... KArgs, class... Args>
+cudaError_t add_kernel_ex(cudaGraphNode_t* out, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+                          void (*f)(KArgs...), dim3 grid, dim3 block, size_t smem, bool cooperative,
+                          Args&&... args) {
+    std::tuple<KArgs...> t(std::forward<Args>(args)...);
+    void* ptrs[sizeof...(KArgs) > 0 ? sizeof...(KArgs) : 1];
+    fill_ptrs(t, ptrs, std::index_sequence_for<KArgs...>{});
+    cudaKernelNodeParams kp{};
+    kp.func = (void*)f;
+    kp.gridDim = grid;
+    kp.blockDim = block;
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = ptrs;
+    kp.extra = nullptr;
+    cudaError_t e = cudaGraphAddKernelNode(out, g, deps.data(), deps.size(), &kp);
+    if (e != cudaSuccess || !cooperative) return e;
+    cudaKernelNodeAttrValue v{};
+    v.cooperative = 1;
+    return cudaGraphKernelNodeSetAttribute(*out, cudaKernelNodeAttributeCooperative, &v);
+}
+
 cudaError_t add_while(cudaGraphNode_t* out, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
                       cudaGraphConditionalHandle h, cudaGraph_t* body) {
     cudaGraphNodeParams np{};
@@ -169,6 +206,60 @@ template <>
 SorCoef<double> sor_coef<double>(ntcfd_ctx* ctx) { return ctx->scd; }
 template <>
 SorCoef<float> sor_coef<float>(ntcfd_ctx* ctx) { return ctx->scf; }
+
+// Brick plan of the resident SOR kernel: the split of the (j,k) rows into at
+// most (SM count) bricks that minimises the largest brick, under the shared
+// memory limit (e of both colours for the brick and a one-row halo, plus d
+// when it also fits).  Returns false when no plan fits one CTA per SM.
+template <class Tc>
+bool plan_resident(ntcfd_ctx* ctx) {
+    const Geom& g = ctx->g;
+    const int mx = ((g.nx + 3) >> 1) + 1;
+    const size_t limit = ctx->smem_optin > 4096 ? ctx->smem_optin - 4096 : 0;
+    long long best = -1;
+    Brick bb{};
+    size_t bsm = 0;
+    for (int nbk = 1; nbk <= g.nz; ++nbk) {
+        const int KB = (g.nz + nbk - 1) / nbk;
+        const int nbk_eff = (g.nz + KB - 1) / KB;
+        for (int nbj = 1; nbj <= g.ny; ++nbj) {
+            const int JB = (g.ny + nbj - 1) / nbj;
+            const int nbj_eff = (g.ny + JB - 1) / JB;
+            if ((long long)nbj_eff * nbk_eff > ctx->sm_count) continue;
+            Brick b{nbj_eff, nbk_eff, JB, KB, mx, 0, 0};
+            if (resident_smem<Tc>(b, g.nx) > limit) continue;
+            // cache d, then rd, when they fit as well
+            b.cache_d = 1;
+            if (resident_smem<Tc>(b, g.nx) > limit) b.cache_d = 0;
+            b.cache_rd = 1;
+            if (resident_smem<Tc>(b, g.nx) > limit) b.cache_rd = 0;
+            const long long cells = (long long)JB * KB;
+            // smallest brick first, then the more cached arrays, then the smaller halo
+            const long long score = cells * 1000000LL + (2 - b.cache_d - b.cache_rd) * 10000LL + (JB + KB);
+            if (best < 0 || score < best) {
+                best = score;
+                bb = b;
+                bsm = resident_smem<Tc>(b, g.nx);
+            }
+        }
+    }
+    if (best < 0) return false;
+    auto kern = k_sor_resident<Tc, kResNT>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kResNT, bsm) != cudaSuccess ||
+        per_sm < 1 || (long long)bb.nbj * bb.nbk > (long long)per_sm * ctx->sm_count) {
+        cudaGetLastError();
+        return false;
+    }
+    ctx->brick = bb;
+    ctx->res_smem = bsm;
+    ctx->res_grid = bb.nbj * bb.nbk;
+    return true;
+}
 
 // The step graph:
 //   [K1 smag] -> K2 predictor -> K3a rhs -> begin -> WHILE(outer){ defect ->
@@ -205,13 +296,34 @@ int build_graph(ntcfd_ctx* ctx) {
     cudaGraph_t outer;
     GK(add_while(&n, G, dep, hout, &outer));
     dep = {n};
-    {
+    ctx->resident = false;
+    if (P.sor_path != NTCFD_SOR_STREAMING) {
+        ctx->resident = plan_resident<Tc>(ctx);
+        if (!ctx->resident && P.sor_path == NTCFD_SOR_RESIDENT)
+            return fail(ctx, NTCFD_EINVAL, "the resident SOR kernel does not fit this grid on this device");
+    }
+    if (ctx->resident) {
+        std::vector<cudaGraphNode_t> od;
+        cudaGraphNode_t m;
+        Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+        GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
+                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, (cudaGraphConditionalHandle)0, 0,
+                      ctx->ring, (unsigned int*)ctx->bar));
+        od = {m};
+        GK(add_kernel_ex(&m, outer, od, k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid), dim3(kResNT),
+                         ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, eR, eB,
+                         (const Tc*)dR, (const Tc*)dB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
+                         ctx->bar, P.omega, P.zeta, P.itmax, ctx->cycle_len, ctx->csweeps, ctx->ring));
+        od = {m};
+        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+    } else {
         GK(cudaGraphConditionalHandleCreate(&hin, outer, 0, 0));
         std::vector<cudaGraphNode_t> od;
         cudaGraphNode_t m;
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
         GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
-                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, hin, 1));
+                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, hin, 1,
+                      (unsigned long long*)nullptr, (unsigned int*)nullptr));
         od = {m};
         cudaGraph_t inner;
         GK(add_while(&m, outer, od, hin, &inner));
@@ -222,18 +334,22 @@ int build_graph(ntcfd_ctx* ctx) {
             const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
             const dim3 bs(kSweepBx, kSweepBy, 1);
             const int half = (g.nx + 1) / 2;
-            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy, g.nz);
+            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
+                          (g.nz + kSweepKpt - 1) / kSweepKpt);
+            const Ctl* cctl = ctx->ctl;
             for (int sub = 0; sub < ctx->csweeps; ++sub) {
-                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy>, gs, bs, g, sc, eR,
-                              (const Tc*)eB, (const Tc*)dR, 0, P.omega, ctx->ctl, sub, P.itmax,
-                              ctx->cycle_len, ctx->slots));
+                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt>, gs, bs, g, sc,
+                              eR, (const Tc*)eB, (const Tc*)dR, (const Tc*)ctx->rdR, 0, P.omega, cctl,
+                              sub, P.itmax,
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
                 id = {s};
-                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy>, gs, bs, g, sc, eB,
-                              (const Tc*)eR, (const Tc*)dB, 1, P.omega, ctx->ctl, sub, P.itmax,
-                              ctx->cycle_len, ctx->slots));
+                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt>, gs, bs, g, sc,
+                              eB, (const Tc*)eR, (const Tc*)dB, (const Tc*)ctx->rdB, 1, P.omega, cctl,
+                              sub, P.itmax,
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
                 id = {s};
             }
-            GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(1), ctx->ctl, ctx->slots,
+            GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(32), ctx->ctl, ctx->slots,
                           ctx->csweeps, P.itmax, ctx->cycle_len, P.zeta, hin));
         }
         GK(add_kernel(&m, outer, od, k_correct<Tc>, g3, b3, g, ctx->p, (const Tc*)eR, (const Tc*)eB));
@@ -270,7 +386,7 @@ int build_graph(ntcfd_ctx* ctx) {
     }
     const int fixed = 10 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->csweeps));
+                  P.diag_divergence, fixed, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
     GK(cudaGraphInstantiate(&ctx->exec, G, 0));
     return 0;
 }
@@ -287,6 +403,7 @@ int validate(const ntcfd_params* p, std::string* why) {
     if (p->sor_order != NTCFD_SOR_REDBLACK)
         return bad("the device solver is red-black SOR (sor_order = NTCFD_SOR_REDBLACK)");
     if (p->scheme != NTCFD_QUICK_CENTRE) return bad("scheme must be NTCFD_QUICK_CENTRE");
+    if (p->sor_path < NTCFD_SOR_AUTO || p->sor_path > NTCFD_SOR_RESIDENT) return bad("bad sor_path");
     if (p->smag_mode != NTCFD_SMAG_REF_ALIASED && p->smag_mode != NTCFD_SMAG_STAGGERED) return bad("bad smag_mode");
     if (p->LES != 0 && p->LES != 1) return bad("LES must be 0 or 1");
     if (p->check_every < 0 || p->mixed_cycle < 0) return bad("check_every and mixed_cycle must be >= 0");
@@ -376,21 +493,46 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
     if ((rc = timed([&] {
              k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
-                                                      ctx->ctl, 0, 0);
+                                                      ctx->ctl, 0, 0, nullptr, nullptr);
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
     const dim3 bs(kSweepBx, kSweepBy, 1);
     const int half = (g.nx + 1) / 2;
-    const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy, g.nz);
+    const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
+                  (g.nz + kSweepKpt - 1) / kSweepKpt);
     const int big = 1 << 30;
     if ((rc = timed([&] {
-             k_sweep<Tc, kSweepBx * kSweepBy><<<gs, bs, 0, ctx->stream>>>(
-                 g, sc, eR, eB, dR, 0, P.omega, ctx->ctl, 0, big, big, ctx->slots);
-             k_sweep<Tc, kSweepBx * kSweepBy><<<gs, bs, 0, ctx->stream>>>(
-                 g, sc, eB, eR, dB, 1, P.omega, ctx->ctl, 0, big, big, ctx->slots);
+             k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, ctx->stream>>>(
+                 g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
+             k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, ctx->stream>>>(
+                 g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
          }, &out->sweep_ms, 2)))
         return rc;
+    // the resident kernel: one launch of `nsw` sweeps (zeta = 0) on a scratch copy of p
+    if (ctx->resident) {
+        const int nsw = 50;
+        double* pscratch = ctx->us;   // rewritten by the predictor every step
+        CK(cudaMemcpyAsync(pscratch, ctx->p, ctx->nat_elems * sizeof(double), cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+        if ((rc = timed([&] {
+                 k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, pscratch, ctx->b, dR, dB, eR, eB,
+                                                          ctx->ctl, 0, 0, ctx->ring, (unsigned int*)ctx->bar);
+                 int zero = 0;
+                 (void)zero;
+                 cudaMemsetAsync(&ctx->ctl->ik, 0, sizeof(int), ctx->stream);
+                 void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&eR,
+                                 (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
+                                 (void*)&ctx->ctl, (void*)&ctx->bar,
+                                 (void*)&P.omega, (void*)&kZeroZeta, (void*)&nsw, (void*)&nsw,
+                                 (void*)&kOne, (void*)&ctx->ring};
+                 cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
+                                             dim3(kResNT), args, ctx->res_smem, ctx->stream);
+             }, &out->resident_ms, 1)))
+            return rc;
+        out->resident_ms -= out->defect_ms;
+        out->resident_sweeps = (float)nsw;
+    }
     // K4 on the predicted velocity in place (us/vs/ws are rewritten every step)
     ProjArgs pj{ctx->us, ctx->vs, ctx->ws, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
@@ -485,7 +627,7 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
         if ((rc = dalloc(ctx, a, N))) return rc;
     if (P.LES && (rc = dalloc(ctx, &ctx->nut, N))) return rc;
     const size_t esz = P.precision == NTCFD_MIXED ? sizeof(float) : sizeof(double);
-    void** spl[] = {&ctx->eR, &ctx->eB, &ctx->dR, &ctx->dB};
+    void** spl[] = {&ctx->eR, &ctx->eB, &ctx->dR, &ctx->dB, &ctx->rdR, &ctx->rdB};
     for (void** a : spl) {
         char* q;
         if ((rc = dalloc(ctx, &q, ctx->spl_elems * esz))) return rc;
@@ -505,8 +647,17 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
     if ((rc = dalloc(ctx, &ctx->faceF, (size_t)P.nx * P.ny))) return rc;
     if ((rc = dalloc(ctx, &ctx->outbuf, 4 * (size_t)P.nx * P.ny * P.nz))) return rc;
     if ((rc = dalloc(ctx, &ctx->ctl, 1))) return rc;
-    if ((rc = dalloc(ctx, &ctx->slots, 64))) return rc;
+    if ((rc = dalloc(ctx, &ctx->slots, 64 * kSpread))) return rc;
     if ((rc = dalloc(ctx, &ctx->divslot, 1))) return rc;
+    if ((rc = dalloc(ctx, &ctx->bar, 1))) return rc;
+    if ((rc = dalloc(ctx, &ctx->ring, 4))) return rc;
+    {
+        int v = 0;
+        CK(cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, P.device));
+        ctx->sm_count = v;
+        CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.device));
+        ctx->smem_optin = (size_t)v;
+    }
     if ((rc = dalloc(ctx, &ctx->coordbuf, (size_t)(P.ny + 5) + (P.nz + 5) + 8))) return rc;
     ctx->coordY = ctx->coordbuf + 1;                  // Y[j] valid for j = -1..ny+3
     ctx->coordZ = ctx->coordbuf + (P.ny + 5) + 4 + 1;
@@ -600,6 +751,14 @@ int ntcfd_set_metrics(ntcfd_ctx* ctx, const double* iDx, const double* Dxs, cons
         const float* tf = F + o_tab[ax];
         ctx->tpd.ax[ax] = AxisTabs<double>{tb, tb + Lx, tb + 2 * Lx, tb + 3 * Lx, tb + 4 * Lx, tb + 5 * Lx};
         ctx->tpf.ax[ax] = AxisTabs<float>{tf, tf + Lx, tf + 2 * Lx, tf + 3 * Lx, tf + 4 * Lx, tf + 5 * Lx};
+    }
+    {
+        const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+        if (ctx->prm.precision == NTCFD_MIXED)
+            k_make_rd<float><<<g3, b3, 0, ctx->stream>>>(g, ctx->scf, (float*)ctx->rdR, (float*)ctx->rdB);
+        else
+            k_make_rd<double><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, (double*)ctx->rdR, (double*)ctx->rdB);
+        CK(cudaGetLastError());
     }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->metrics_set = true;
@@ -742,7 +901,8 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     int status = 0;
     for (int s = 0; s < nsteps; ++s) {
         ctx->time = ctx->time + ctx->prm.dt;   // main.f90:271
-        if (rec[s].nonfinite) status = NTCFD_ENONFINITE;
+        if (rec[s].timeout) status = NTCFD_ETIMEOUT;
+        else if (rec[s].nonfinite && status != NTCFD_ETIMEOUT) status = NTCFD_ENONFINITE;
         else if (!rec[s].converged && status == 0) status = NTCFD_NOT_CONVERGED;
         if (info) {
             ntcfd_step_info& I = info[s];
@@ -755,9 +915,11 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
             I.div_max = rec[s].divmax;
             I.dc_cycles = rec[s].cycles;
             I.launches = rec[s].launches;
+            I.sor_path = ctx->resident ? NTCFD_SOR_RESIDENT : NTCFD_SOR_STREAMING;
         }
     }
-    if (status == NTCFD_ENONFINITE) fail(ctx, status, "non-finite value in the SOR solve");
+    if (status == NTCFD_ETIMEOUT) fail(ctx, status, "the resident SOR kernel's grid barrier gave up waiting");
+    else if (status == NTCFD_ENONFINITE) fail(ctx, status, "non-finite value in the SOR solve");
     else if (status == NTCFD_NOT_CONVERGED) fail(ctx, status, "SOR stopped at itmax in at least one step");
     return status;
 }

@@ -59,7 +59,7 @@ struct Ctl {
     int cycles;                   // defect-correction cycles in this step
     int inner;                    // sweeps done in the current cycle
     int bodies;                   // inner loop bodies run in this step
-    int pad;
+    int timeout;                  // a bounded device wait gave up
     double last_change;           // value of the last tested sweep
     double cdrag, clift, divmax;
 };
@@ -69,23 +69,36 @@ struct StepRec {
     int sor_iters, converged;
     double last_change, cdrag, clift, divmax;
     int cycles, nonfinite;
-    int launches, pad;
+    int launches, timeout;
 };
 
 __device__ __forceinline__ unsigned long long dbits(double x) {
     return (unsigned long long)__double_as_longlong(x);
 }
 
-// Block-wide max of a non-negative double, then one atomicMax on its bit
-// pattern (ordered like the value for non-negative doubles; NaN patterns of
-// either sign compare above +Inf after clearing the sign bit).
-template <int NT>
-__device__ __forceinline__ void block_max_atomic(double v, unsigned long long* dst) {
-    __shared__ unsigned long long red[NT / 32];
-    unsigned long long b = dbits(v) & 0x7fffffffffffffffULL;
+// Order-preserving bit patterns of |x|: for non-negative IEEE values the
+// unsigned pattern orders like the value, and every NaN pattern lies above
+// +Inf, so a max over patterns also detects non-finite values.
+__device__ __forceinline__ unsigned long long abs_bits(double x) {
+    return dbits(x) & 0x7fffffffffffffffULL;
+}
+__device__ __forceinline__ unsigned int abs_bits(float x) {
+    return __float_as_uint(x) & 0x7fffffffu;
+}
+__device__ __forceinline__ unsigned long long widen_bits(unsigned long long b) { return b; }
+__device__ __forceinline__ unsigned long long widen_bits(unsigned int b) {
+    return dbits((double)__uint_as_float(b));   // float -> double keeps order, Inf and NaN
+}
+
+// Block-wide max of order-preserving patterns b (see abs_bits), then one
+// atomicMax of the double pattern on *dst.  NT = threads per block;
+// blockDim.x must be a multiple of 32.
+template <int NT, class B>
+__device__ __forceinline__ void block_max_bits(B b, unsigned long long* dst) {
+    __shared__ B red[NT / 32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+        const B t = __shfl_xor_sync(0xffffffffu, b, o);
         b = t > b ? t : b;
     }
     const int lane = threadIdx.x & 31;
@@ -93,15 +106,24 @@ __device__ __forceinline__ void block_max_atomic(double v, unsigned long long* d
     if (lane == 0) red[warp] = b;
     __syncthreads();
     if (warp == 0) {
-        b = (lane < NT / 32) ? red[lane] : 0ULL;
+        b = (lane < NT / 32) ? red[lane] : B(0);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
-            unsigned long long t = __shfl_xor_sync(0xffffffffu, b, o);
+            const B t = __shfl_xor_sync(0xffffffffu, b, o);
             b = t > b ? t : b;
         }
-        if (lane == 0 && b != 0ULL) atomicMax(dst, b);
+        if (lane == 0 && b != B(0)) atomicMax(dst, widen_bits(b));
     }
 }
+
+template <int NT, class T>
+__device__ __forceinline__ void block_max_atomic(T v, unsigned long long* dst) {
+    block_max_bits<NT>(abs_bits(v), dst);
+}
+
+// Per-sweep maxima are spread over kSpread slots (by block index) so that
+// thousands of blocks do not serialise on one address.
+constexpr int kSpread = 32;
 
 constexpr unsigned long long kInfBits = 0x7ff0000000000000ULL;
 

@@ -204,4 +204,4 @@ class Solver:
         t = abi.NtcfdKernelTimes()
         self._check(self.lib.ntcfd_time_kernels(self.h, reps, ctypes.byref(t)))
         return {n: getattr(t, n) for n in ("predictor_ms", "rhs_ms", "defect_ms", "sweep_ms",
-                                           "project_ms", "bc_ms")}
+                                           "project_ms", "bc_ms", "resident_ms", "resident_sweeps")}

@@ -25,9 +25,15 @@ _IP = ctypes.POINTER(ctypes.c_int)
 
 
 def build(force: bool = False) -> str:
-    """Compiles the oracle with its Makefile (g++ -fopenmp)."""
-    if force or not os.path.exists(LIB):
-        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    """Compiles the oracle with its Makefile (g++ -fopenmp); make rebuilds
+    when the sources or include/ntcfd.h (the shared structs) changed.  On a
+    machine without the compiler the prebuilt library is used as it is."""
+    args = ["make", "-C", HERE] + (["-B"] if force else [])
+    try:
+        subprocess.run(args, check=True, capture_output=True)
+    except (FileNotFoundError, subprocess.CalledProcessError):
+        if force or not os.path.exists(LIB):
+            raise
     return LIB
 
 

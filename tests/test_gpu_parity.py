@@ -13,7 +13,8 @@ import pytest
 from conftest import interior, rel_l2
 from ntustcfdlab_b200 import abi
 from ntustcfdlab_b200.abi import (FP64, MIXED, SMAG_REF_ALIASED, SMAG_STAGGERED, SOR_LEX,
-                                  SOR_REDBLACK, f4, make_params, params_copy)
+                                  SOR_REDBLACK, SOR_RESIDENT, SOR_STREAMING, f4, make_params,
+                                  params_copy)
 
 pytestmark = pytest.mark.gpu
 
@@ -77,15 +78,17 @@ def test_boundary_conditions_exact(orc, bcname):
         np.testing.assert_array_equal(a, o.get(k), err_msg=k)
 
 
+@pytest.mark.parametrize("path", [SOR_STREAMING, SOR_RESIDENT])
 @pytest.mark.parametrize("bcname", list(BCS))
 @pytest.mark.parametrize("sweeps", [0, 7])
-def test_one_step_forced_sweeps(orc, bcname, sweeps):
-    """A full loop body with a fixed sweep count (itmax = sweeps, zeta = 0)."""
+def test_one_step_forced_sweeps(orc, bcname, sweeps, path):
+    """A full loop body with a fixed sweep count (itmax = sweeps, zeta = 0),
+    through both device SOR paths."""
     n = (13, 11, 9)
     g = orc.gridder_unequal(*n, 1.0, 1.3, 1.7,
                             (12.5, 0.65, 0.6, 16, 4, 6, 4, 6, 1.0, 0.1, 0.3, 0.2, 0.5))
     p = make_params(*n, Re=100.0, dt=f4(1e-3), zeta=0.0, itmax=sweeps, bc=BCS[bcname],
-                    bc_value={"Back": (0.3, -0.2, 1.0)})
+                    bc_value={"Back": (0.3, -0.2, 1.0)}, sor_path=path)
     s, o = _pair(orc, p, g, _random_state((17, 15, 13), 5))
     info, rc = s.step(1)
     oi = o.step(1, forced=[sweeps])
@@ -106,8 +109,23 @@ def test_les_step_parity(orc, mode):
     _compare(s, o, 1e-12)
 
 
-def test_c1_cavity_parity():
-    pass
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_streaming_and_resident_paths_agree(prec):
+    """The two device SOR paths run the same red-black iteration and stop rule."""
+    from ntustcfdlab_b200 import cases
+    res = {}
+    for path in (SOR_STREAMING, SOR_RESIDENT):
+        c = cases.cavity(48, 1000.0, 5e-4, 30, precision=prec)
+        s = _solver(params_copy(c.params, sor_path=path, mixed_cycle=8), c.grid)
+        s.boundary_conditions()
+        info, rc = s.step(c.steps)
+        assert rc == 0 and all(i.sor_path == path for i in info)
+        res[path] = (s.get_state(), [i.sor_iters for i in info], [i.dc_cycles for i in info])
+        s.close()
+    a, b = res[SOR_STREAMING], res[SOR_RESIDENT]
+    assert a[1] == b[1] and a[2] == b[2]
+    for k, x, y in zip(FIELDS, a[0], b[0]):
+        assert rel_l2(interior(x), interior(y)) <= 1e-12, k
 
 
 @pytest.fixture(scope="module")
