@@ -48,6 +48,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cycle", type=int, default=8,
+                    help="mixed path: FP32 sweeps per FP64 defect-correction cycle")
+    ap.add_argument("--eager", action="store_true",
+                    help="launch kernels one by one instead of CUDA graphs (for ncu)")
+    ap.add_argument("--sor-path", choices=("auto", "streaming", "resident"), default="auto")
+    ap.add_argument("--no-roofline", action="store_true", help="skip the standalone kernel timing")
     return ap.parse_args()
 
 
@@ -133,10 +139,13 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ our arm
-def cavity_case(n, precision, device):
+def cavity_case(n, precision, device, args):
     from ntustcfdlab_b200 import cases
     c = cases.cavity(n, 1000.0, 5e-4, 500, precision=precision)
     c.params.device = device
+    c.params.mixed_cycle = args.cycle if precision == 1 else 0
+    c.params.eager = 1 if args.eager else 0
+    c.params.sor_path = {"auto": 0, "streaming": 1, "resident": 2}[args.sor_path]
     return c
 
 
@@ -238,14 +247,21 @@ def cpu_baseline_from(s_gpu, case, seconds):
     return case.cells * steps / el / 1e6, threads, steps, sweeps, el
 
 
-def roofline(s, case, reps=20):
-    """Dominant kernel: the half-sweep of the SOR solve.  Algorithmic bytes
-    per half-sweep launch: 3 S per cell per full red+black sweep (read e and
-    d, write e; S = 4 B in mixed, 8 B in FP64), i.e. 1.5 S per cell per launch."""
+def roofline(s, case, path, reps=20):
+    """Dominant kernel: the SOR sweeps.  Algorithmic bytes: 3 S per cell per
+    full red+black sweep (read e and d, write e; S = 4 B mixed, 8 B FP64).
+    Streaming path: one launch = one colour = 1.5 S per cell.  Resident path:
+    one launch runs `resident_sweeps` sweeps (timed standalone, zeta = 0)."""
     kt = s.time_kernels(reps)
     S = 4 if case.params.precision == 1 else 8
-    alg = 1.5 * S * case.cells
-    ms = kt["sweep_ms"]
+    if path == 2 and kt["resident_ms"] > 0:
+        kernel = "k_sor_resident (all sweeps of a correction cycle, e in shared memory)"
+        alg = 3 * S * case.cells * kt["resident_sweeps"]
+        ms = kt["resident_ms"]
+    else:
+        kernel = "k_sweep (one colour of a red-black SOR sweep)"
+        alg = 1.5 * S * case.cells
+        ms = kt["sweep_ms"]
     ach = alg / (ms * 1e-3) / 1e9
     peaks = {}
     try:
@@ -254,16 +270,16 @@ def roofline(s, case, reps=20):
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     traffic = None
-    tp = os.path.join(ROOT, "profiles", "sweep_traffic.json")
+    tp = os.path.join(ROOT, "profiles", "sor_traffic.json")
     if os.path.exists(tp):
         try:
             tr = json.load(open(tp))
-            if tr.get("cells") == case.cells and tr.get("bytes_per_element") == S:
-                traffic = tr.get("dram_bytes_per_launch")
+            key = f"{case.params.nx}:{S}:{path}"
+            if key in tr:
+                traffic = tr[key]["dram_bytes_per_launch"]
         except Exception:
             traffic = None
-    return {"kernel": "k_sweep (one colour of a red-black SOR sweep)", "bound": "hbm",
-            "achieved": round(ach, 1), "peak": peak,
+    return {"kernel": kernel, "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
             "unit": "GB/s", "frac": round(ach / peak, 3), "traffic": traffic,
             "algorithmic_bytes_per_launch": alg, "avg_launch_ms": ms,
@@ -288,7 +304,7 @@ def run_ours(args):
                                 device_id=torch.device("cuda", local))
     from ntustcfdlab_b200.abi import FP64, MIXED
     K, W = args.steps, max(args.warmup, 0)
-    mixed = cavity_case(args.n, MIXED, local)
+    mixed = cavity_case(args.n, MIXED, local, args)
     s, info, rc, ms, clocks = timed_run(mixed, K, W, sampler_index=local)
     ms_max = aggregate(ms, "max")
     cells_total = mixed.cells * world
@@ -297,7 +313,7 @@ def run_ours(args):
     launches = int(sum(i.launches for i in info))
     extra = {}
     if not args.no_fp64:
-        f64 = cavity_case(args.n, FP64, local)
+        f64 = cavity_case(args.n, FP64, local, args)
         s64, info64, _, ms64, _ = timed_run(f64, K, W)
         ms64_max = aggregate(ms64, "max")
         v64 = cells_total * K / (ms64_max * 1e-3) / 1e6
@@ -314,7 +330,8 @@ def run_ours(args):
         e2e = {"value": round(cells_total * K / t_max / 1e6, 2), "unit": UNIT,
                "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
                "timing": "host wall clock around the synchronous C-ABI calls"}
-    rl = roofline(s, mixed) if rank == 0 else None
+    path = info[0].sor_path if info else 1
+    rl = roofline(s, mixed, path) if rank == 0 and not args.no_roofline else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, thr, nst, nsw, el = cpu_baseline_from(s, mixed, args.cpu_seconds)
@@ -329,7 +346,10 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (lid-driven cavity from rest, no dataset)",
             "config": {"workload": f"lid-driven cavity {args.n}^3, Re=1000, dt=5e-4, zeta=1e-4, "
-                                   f"mixed precision (FP32 red-black SOR + FP64 defect correction)",
+                                   f"mixed precision (FP32 red-black SOR + FP64 defect correction "
+                                   f"every {args.cycle} sweeps)",
+                       "sor_path": {1: "streaming", 2: "resident"}.get(path, str(path)),
+                       "launch": "eager" if args.eager else "cuda-graph",
                        "grid": [args.n] * 3, "case_steps": 500,
                        "l2": "inputs larger than L2: state is 9 FP64 arrays of "
                              f"{(args.n + 4) ** 3 * 8 / 1e6:.0f} MB, no flush",

@@ -84,7 +84,9 @@ typedef struct ntcfd_params {
     int diag_divergence;     /* 1: report max|div u^{n+1}| in ntcfd_step_info.div_max */
     int device;              /* CUDA device ordinal that holds the grid */
     int sor_path;            /* NTCFD_SOR_AUTO, NTCFD_SOR_STREAMING or NTCFD_SOR_RESIDENT */
-    int reserved[4];         /* must be zero */
+    int eager;               /* 1: launch the step's kernels one by one from the host (no
+                                CUDA graph; for kernel profilers and debugging, slower) */
+    int reserved[3];         /* must be zero */
 } ntcfd_params;
 
 typedef struct ntcfd_step_info {

@@ -55,7 +55,8 @@ class NtcfdParams(ctypes.Structure):
         ("diag_divergence", ctypes.c_int),
         ("device", ctypes.c_int),
         ("sor_path", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("eager", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 
@@ -86,7 +87,7 @@ def make_params(nx, ny, nz, *, Re, dt, omega=1.5, zeta=f4(1e-4), itmax=3000, LES
                 Cs=f4(0.18), precision=FP64, sor_order=SOR_REDBLACK,
                 smag_mode=SMAG_REF_ALIASED, check_every=1, bc=None, bc_value=None,
                 u_solid=(0.0, 0.0, 0.0), lx=1.0, mixed_cycle=0,
-                diag_divergence=0, device=0, sor_path=SOR_AUTO) -> NtcfdParams:
+                diag_divergence=0, device=0, sor_path=SOR_AUTO, eager=0) -> NtcfdParams:
     """Builds an ``ntcfd_params``.  ``bc`` maps wall name -> (u, v, w) kind
     strings; missing walls are no-slip, as in variables_module.f90:110-132."""
     p = NtcfdParams()
@@ -110,6 +111,7 @@ def make_params(nx, ny, nz, *, Re, dt, omega=1.5, zeta=f4(1e-4), itmax=3000, LES
     p.diag_divergence = diag_divergence
     p.device = device
     p.sor_path = sor_path
+    p.eager = eager
     return p
 
 

@@ -166,8 +166,9 @@ __global__ void __launch_bounds__(NT) k_sweep(Geom g, SorCoef<Tc> sc, Tc* __rest
 }
 
 // One warp: the max over the kSpread slots of that sweep is its max|change|.
+// Outside a graph (in_graph = 0) the host reads ctl and takes the decision.
 __global__ void k_sor_check(Ctl* ctl, unsigned long long* slots, int csweeps, int itmax,
-                            int cycle_len, double zeta, cudaGraphConditionalHandle inner) {
+                            int cycle_len, double zeta, cudaGraphConditionalHandle inner, int in_graph) {
     const int lane = threadIdx.x;
     const int ik = ctl->ik, in = ctl->inner;
     int ran = csweeps;
@@ -192,7 +193,8 @@ __global__ void k_sor_check(Ctl* ctl, unsigned long long* slots, int csweeps, in
     if (nonfinite) ctl->nonfinite = 1;
     if (conv) ctl->converged = 1;
     const bool stop = conv || nonfinite || ctl->ik >= itmax || ctl->inner >= cycle_len || ran == 0;
-    cudaGraphSetConditional(inner, stop ? 0u : 1u);
+    ctl->pad_stop = stop ? 1 : 0;
+    if (in_graph) cudaGraphSetConditional(inner, stop ? 0u : 1u);
 }
 
 // p += e over the interior (natural <- colour-split).
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(256) k_correct(Geom g, double* p, const Tc* eR
 }
 
 // Start of a solve: counters reset, outer loop armed when itmax > 0.
-__global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer) {
+__global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer, int in_graph) {
     ctl->ik = 0;
     ctl->inner = 0;
     ctl->cycles = 0;
@@ -217,15 +219,16 @@ __global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle oute
     ctl->converged = 0;
     ctl->nonfinite = 0;
     ctl->last_change = 0.0;
-    cudaGraphSetConditional(outer, itmax > 0 ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(outer, itmax > 0 ? 1u : 0u);
 }
 
 // End of a defect-correction cycle: another cycle only when the inner loop
 // stopped on its cycle length.
-__global__ void k_outer_check(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer) {
+__global__ void k_outer_check(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer, int in_graph) {
     ctl->cycles += 1;
     const bool more = !ctl->converged && !ctl->nonfinite && !ctl->timeout && ctl->ik < itmax;
-    cudaGraphSetConditional(outer, more ? 1u : 0u);
+    ctl->pad_more = more ? 1 : 0;
+    if (in_graph) cudaGraphSetConditional(outer, more ? 1u : 0u);
 }
 
 }  // namespace ntcfd

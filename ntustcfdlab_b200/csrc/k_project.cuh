@@ -76,54 +76,65 @@ __global__ void k_force_columns(Geom g, const double* partZ, const double* partY
     }
 }
 
+// Guarded j-sums (virtualForceIntegrator.f90:45-57): one warp per i, lanes
+// over j, fixed-order shuffle reduction; FXy(i), FYy(i) to global.  The last
+// block to finish (counter in ctl) does the guarded i-sum (60-76) in one
+// block with a fixed-order tree, then cDrag and cLift (80-81).
 template <int NT>
 __global__ void __launch_bounds__(NT) k_force_total(Geom g, const double* FXz, const double* FYz,
-                                                    double lx, Ctl* ctl, StepRec* rec) {
-    __shared__ double sx[NT], sy[NT];
+                                                    double* FXy, double* FYy, double lx, Ctl* ctl,
+                                                    unsigned int* done, StepRec* rec) {
     const int nx = g.nx, ny = g.ny;
-    // pass 1: guarded j-sums, one thread per i (strided), kept in global scratch via smem tiles
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (NT / 32) + (threadIdx.x >> 5) + 1;
+    if (i <= nx) {
+        double ax = 0.0, ay = 0.0;
+        for (int j = lane + 1; j <= ny; j += 32) {
+            const long long q = (long long)(j - 1) * nx + (i - 1);
+            const double cx = FXz[q], cy = FYz[q];
+            const double xm = (j > 1) ? FXz[q - nx] : 0.0, xp = (j < ny) ? FXz[q + nx] : 0.0;
+            const double ym = (j > 1) ? FYz[q - nx] : 0.0, yp = (j < ny) ? FYz[q + nx] : 0.0;
+            if (cx != 0.0) ax += (xm * g.Dys[j - 1] + 4.0 * cx * g.Dys[j] + xp * g.Dys[j + 1]) / 6.0;
+            if (cy != 0.0) ay += (ym * g.Dys[j - 1] + 4.0 * cy * g.Dys[j] + yp * g.Dys[j + 1]) / 6.0;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        }
+        if (lane == 0) { FXy[i - 1] = ax; FYy[i - 1] = ay; }
+    }
+    // last block: the i-sum
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        last = atomicAdd(done, 1u) + 1u == gridDim.x;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sx[NT], sy[NT];
     double tx = 0.0, ty = 0.0;
-    for (int i0 = 0; i0 < nx; i0 += NT) {
-        // FXy/FYy for i in [i0-1, i0+NT] are needed by this tile's terms
-        __shared__ double fxy[NT + 2], fyy[NT + 2];
-        for (int t = threadIdx.x; t < NT + 2; t += NT) {
-            const int i = i0 + t;  // 1-based i = i0 + t  (t=0 -> i0, the left neighbour)
-            double ax = 0.0, ay = 0.0;
-            if (i >= 1 && i <= nx) {
-                for (int j = 1; j <= ny; ++j) {
-                    const long long q = (long long)(j - 1) * nx + (i - 1);
-                    const double cx = FXz[q], cy = FYz[q];
-                    const double xm = (j > 1) ? FXz[q - nx] : 0.0, xp = (j < ny) ? FXz[q + nx] : 0.0;
-                    const double ym = (j > 1) ? FYz[q - nx] : 0.0, yp = (j < ny) ? FYz[q + nx] : 0.0;
-                    if (cx != 0.0) ax = ax + (xm * g.Dys[j - 1] + 4.0 * cx * g.Dys[j] + xp * g.Dys[j + 1]) / 6.0;
-                    if (cy != 0.0) ay = ay + (ym * g.Dys[j - 1] + 4.0 * cy * g.Dys[j] + yp * g.Dys[j + 1]) / 6.0;
-                }
-            }
-            fxy[t] = ax;
-            fyy[t] = ay;
-        }
-        __syncthreads();
-        const int i = i0 + 1 + threadIdx.x;
-        if (i <= nx) {
-            const double c = fxy[threadIdx.x + 1], cyv = fyy[threadIdx.x + 1];
-            const double l = fxy[threadIdx.x], r = (i < nx) ? fxy[threadIdx.x + 2] : 0.0;
-            const double ly = fyy[threadIdx.x], ry = (i < nx) ? fyy[threadIdx.x + 2] : 0.0;
-            if (c != 0.0) tx += (l * g.Dxs[i - 1] + 4.0 * c * g.Dxs[i] + r * g.Dxs[i + 1]) / 6.0;
-            if (cyv != 0.0) ty += (ly * g.Dxs[i - 1] + 4.0 * cyv * g.Dxs[i] + ry * g.Dxs[i + 1]) / 6.0;
-        }
-        __syncthreads();
+    for (int ii = threadIdx.x + 1; ii <= nx; ii += NT) {
+        const double c = __ldcg(FXy + ii - 1), cyv = __ldcg(FYy + ii - 1);
+        const double l = ii > 1 ? __ldcg(FXy + ii - 2) : 0.0, r = ii < nx ? __ldcg(FXy + ii) : 0.0;
+        const double ly = ii > 1 ? __ldcg(FYy + ii - 2) : 0.0, ry = ii < nx ? __ldcg(FYy + ii) : 0.0;
+        if (c != 0.0) tx += (l * g.Dxs[ii - 1] + 4.0 * c * g.Dxs[ii] + r * g.Dxs[ii + 1]) / 6.0;
+        if (cyv != 0.0) ty += (ly * g.Dxs[ii - 1] + 4.0 * cyv * g.Dxs[ii] + ry * g.Dxs[ii + 1]) / 6.0;
     }
     sx[threadIdx.x] = tx;
     sy[threadIdx.x] = ty;
     __syncthreads();
-    for (int s = NT / 2; s > 0; s >>= 1) {
-        if (threadIdx.x < s) {
-            sx[threadIdx.x] += sx[threadIdx.x + s];
-            sy[threadIdx.x] += sy[threadIdx.x + s];
+    for (int st = NT / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) {
+            sx[threadIdx.x] += sx[threadIdx.x + st];
+            sy[threadIdx.x] += sy[threadIdx.x + st];
         }
         __syncthreads();
     }
     if (threadIdx.x == 0) {
+        *done = 0u;
         const int s = ctl->step;
         ctl->cdrag = (-2.0) * sx[0] / lx;
         ctl->clift = (-2.0) * sy[0] / lx;

@@ -64,6 +64,8 @@ struct ntcfd_ctx {
     SorCoef<double> scd{};
     SorCoef<float> scf{};
     double *partZ = nullptr, *partY = nullptr, *FXz = nullptr, *FYz = nullptr;
+    double *FXy = nullptr, *FYy = nullptr;
+    unsigned int* fdone = nullptr;         // block counter of k_force_total
     double *faceW = nullptr, *faceE = nullptr, *faceS = nullptr, *faceN = nullptr;
     double *faceB = nullptr, *faceF = nullptr;
     double* outbuf = nullptr;   // pre, uc, vc, wc
@@ -291,7 +293,7 @@ int build_graph(ntcfd_ctx* ctx) {
     dep = {n};
     cudaGraphConditionalHandle hout, hin;
     GK(cudaGraphConditionalHandleCreate(&hout, G, 0, 0));
-    GK(add_kernel(&n, G, dep, k_sor_begin, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+    GK(add_kernel(&n, G, dep, k_sor_begin, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
     dep = {n};
     cudaGraph_t outer;
     GK(add_while(&n, G, dep, hout, &outer));
@@ -315,7 +317,7 @@ int build_graph(ntcfd_ctx* ctx) {
                          (const Tc*)dR, (const Tc*)dB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
                          ctx->bar, P.omega, P.zeta, P.itmax, ctx->cycle_len, ctx->csweeps, ctx->ring));
         od = {m};
-        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
     } else {
         GK(cudaGraphConditionalHandleCreate(&hin, outer, 0, 0));
         std::vector<cudaGraphNode_t> od;
@@ -350,11 +352,11 @@ int build_graph(ntcfd_ctx* ctx) {
                 id = {s};
             }
             GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(32), ctx->ctl, ctx->slots,
-                          ctx->csweeps, P.itmax, ctx->cycle_len, P.zeta, hin));
+                          ctx->csweeps, P.itmax, ctx->cycle_len, P.zeta, hin, 1));
         }
         GK(add_kernel(&m, outer, od, k_correct<Tc>, g3, b3, g, ctx->p, (const Tc*)eR, (const Tc*)eB));
         od = {m};
-        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout));
+        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
     }
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
@@ -364,8 +366,8 @@ int build_graph(ntcfd_ctx* ctx) {
     GK(add_kernel(&n, G, dep, k_force_columns, dim3(296), dim3(256), g, (const double*)ctx->partZ,
                   (const double*)ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz));
     dep = {n};
-    GK(add_kernel(&n, G, dep, k_force_total<256>, dim3(1), dim3(256), g, (const double*)ctx->FXz,
-                  (const double*)ctx->FYz, P.lx, ctx->ctl, ctx->rec));
+    GK(add_kernel(&n, G, dep, k_force_total<256>, dim3((g.nx + 7) / 8), dim3(256), g, (const double*)ctx->FXz,
+                  (const double*)ctx->FYz, ctx->FXy, ctx->FYy, P.lx, ctx->ctl, ctx->fdone, ctx->rec));
     dep = {n};
     BcArgs ba{};
     ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
@@ -391,6 +393,93 @@ int build_graph(ntcfd_ctx* ctx) {
     return 0;
 }
 
+// One step with every kernel launched from the host (no CUDA graph): the
+// same kernels and loop decisions as the graph, for kernel profilers (which
+// cannot look inside graphs that contain conditional nodes) and debugging.
+template <class Tc>
+int run_step_eager(ntcfd_ctx* ctx) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaStream_t st = ctx->stream;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+    const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
+    if (P.LES)
+        k_smagorinsky<<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
+                                         P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
+    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
+                P.dt, 1. / P.Re, P.LES};
+    k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
+    k_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
+    k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
+    Ctl h{};
+    auto read_ctl = [&]() -> int {
+        CK(cudaMemcpyAsync(&h, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    };
+    bool more = P.itmax > 0;
+    const int big_guard = ctx->csweeps > 1 ? 1 : 0;
+    while (more) {
+        if (ctx->resident) {
+            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB, ctx->ctl, 0, 0,
+                                            ctx->ring, (unsigned int*)ctx->bar);
+            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&ctx->p, (void*)&eR,
+                            (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
+                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&P.zeta,
+                            (void*)&P.itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
+            CK(cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
+                                           dim3(kResNT), args, ctx->res_smem, st));
+        } else {
+            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB, ctx->ctl, 0, 0,
+                                            nullptr, nullptr);
+            const dim3 bs(kSweepBx, kSweepBy, 1);
+            const int half = (g.nx + 1) / 2;
+            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
+                          (g.nz + kSweepKpt - 1) / kSweepKpt);
+            for (;;) {
+                for (int sub = 0; sub < ctx->csweeps; ++sub) {
+                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, sub, P.itmax,
+                        ctx->cycle_len, big_guard, ctx->slots);
+                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, sub, P.itmax,
+                        ctx->cycle_len, big_guard, ctx->slots);
+                }
+                k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, P.itmax, ctx->cycle_len,
+                                              P.zeta, 0, 0);
+                if (int rc = read_ctl()) return rc;
+                if (h.pad_stop) break;
+            }
+            k_correct<Tc><<<g3, b3, 0, st>>>(g, ctx->p, eR, eB);
+        }
+        k_outer_check<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
+        if (int rc = read_ctl()) return rc;
+        more = h.pad_more != 0;
+    }
+    ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
+                ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
+    k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0, st>>>(g, pj);
+    k_force_columns<<<296, 256, 0, st>>>(g, ctx->partZ, ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz);
+    k_force_total<256><<<(g.nx + 7) / 8, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, P.lx,
+                                                          ctx->ctl, ctx->fdone, ctx->rec);
+    BcArgs ba{};
+    ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+    std::memcpy(ba.bc, P.bc, sizeof ba.bc);
+    std::memcpy(ba.val, P.bc_value, sizeof ba.val);
+    ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
+    ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
+    k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+    k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+    k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+    if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
+    const int fixed = 10 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0);
+    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed,
+                                ctx->resident ? 0 : 2 * ctx->csweeps + 1);
+    CK(cudaGetLastError());
+    return 0;
+}
+
 int validate(const ntcfd_params* p, std::string* why) {
     char b[256];
     auto bad = [&](const char* m) { *why = m; return NTCFD_EINVAL; };
@@ -404,6 +493,7 @@ int validate(const ntcfd_params* p, std::string* why) {
         return bad("the device solver is red-black SOR (sor_order = NTCFD_SOR_REDBLACK)");
     if (p->scheme != NTCFD_QUICK_CENTRE) return bad("scheme must be NTCFD_QUICK_CENTRE");
     if (p->sor_path < NTCFD_SOR_AUTO || p->sor_path > NTCFD_SOR_RESIDENT) return bad("bad sor_path");
+    if (p->eager != 0 && p->eager != 1) return bad("eager must be 0 or 1");
     if (p->smag_mode != NTCFD_SMAG_REF_ALIASED && p->smag_mode != NTCFD_SMAG_STAGGERED) return bad("bad smag_mode");
     if (p->LES != 0 && p->LES != 1) return bad("LES must be 0 or 1");
     if (p->check_every < 0 || p->mixed_cycle < 0) return bad("check_every and mixed_cycle must be >= 0");
@@ -639,6 +729,9 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
     if ((rc = dalloc(ctx, &ctx->partY, cols * ctx->nchunk))) return rc;
     if ((rc = dalloc(ctx, &ctx->FXz, cols))) return rc;
     if ((rc = dalloc(ctx, &ctx->FYz, cols))) return rc;
+    if ((rc = dalloc(ctx, &ctx->FXy, (size_t)P.nx))) return rc;
+    if ((rc = dalloc(ctx, &ctx->FYy, (size_t)P.nx))) return rc;
+    if ((rc = dalloc(ctx, &ctx->fdone, 1))) return rc;
     if ((rc = dalloc(ctx, &ctx->faceW, (size_t)P.ny * P.nz))) return rc;
     if ((rc = dalloc(ctx, &ctx->faceE, (size_t)P.ny * P.nz))) return rc;
     if ((rc = dalloc(ctx, &ctx->faceS, (size_t)P.nx * P.nz))) return rc;
@@ -887,12 +980,21 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
         ctx->rec_cap = cap;
     }
     if (!ctx->exec) {
+        // the graph is built in eager mode too: it plans the SOR path
         const int rc = ctx->prm.precision == NTCFD_MIXED ? build_graph<float>(ctx) : build_graph<double>(ctx);
         if (rc) return rc;
     }
     CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (int s = 0; s < nsteps; ++s) CK(cudaGraphLaunch(ctx->exec, ctx->stream));
+    for (int s = 0; s < nsteps; ++s) {
+        if (ctx->prm.eager) {
+            const int rc = ctx->prm.precision == NTCFD_MIXED ? run_step_eager<float>(ctx)
+                                                             : run_step_eager<double>(ctx);
+            if (rc) return rc;
+        } else {
+            CK(cudaGraphLaunch(ctx->exec, ctx->stream));
+        }
+    }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     std::vector<StepRec> rec(nsteps);
     CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));

@@ -269,3 +269,21 @@ def test_nonfinite_state_is_reported():
     with pytest.raises(NtcfdError) as e:
         s.step(1)
     assert e.value.code == abi.NTCFD_ENONFINITE
+
+
+@pytest.mark.parametrize("path", [SOR_STREAMING, SOR_RESIDENT])
+def test_eager_launch_matches_graph(path):
+    """The host-driven launch mode runs the same kernels and loop decisions."""
+    from ntustcfdlab_b200 import cases
+    out = []
+    for eager in (0, 1):
+        c = cases.cavity(32, 400.0, 1e-3, 6, precision=MIXED)
+        s = _solver(params_copy(c.params, sor_path=path, eager=eager, mixed_cycle=4), c.grid)
+        s.boundary_conditions()
+        info, rc = s.step(c.steps)
+        assert rc == 0
+        out.append((s.get_state(), [(i.sor_iters, i.dc_cycles, i.launches) for i in info]))
+        s.close()
+    assert out[0][1] == out[1][1]
+    for a, b in zip(out[0][0], out[1][0]):
+        np.testing.assert_array_equal(a, b)

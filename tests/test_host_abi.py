@@ -39,9 +39,10 @@ def test_ctypes_struct_layout_matches_header(ntcfd_lib):
     assert p.Re == 10.0 and p.dt == f4(1e-3) and p.zeta == f4(1e-4) and p.Cs == f4(0.18)
     assert p.omega == 1.5 and p.itmax == 3000 and p.check_every == 1 and p.lx == 1.0
     assert p.bc[3][2] == abi.BC_DIRICHLET and p.bc[0][0] == abi.BC_NOSLIP
-    assert list(p.reserved) == [0] * 4 and p.device == 0 and p.sor_path == abi.SOR_AUTO
+    assert list(p.reserved) == [0] * 3 and p.device == 0 and p.sor_path == abi.SOR_AUTO
+    assert p.eager == 0
     # C layout of ntcfd_params on x86-64: 3 ints (+pad), 4 doubles, 2 ints, 1 double,
-    # 5 ints, int[6][3], double[6][3], double[3], double, 4 ints, int[4]
+    # 5 ints, int[6][3], double[6][3], double[3], double, 5 ints, int[3]
     assert ctypes.sizeof(NtcfdParams) == 368
 
 
