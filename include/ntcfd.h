@@ -203,6 +203,62 @@ int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms);
  * and ETA of the context are left unchanged. */
 int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
 
+/* ------------------------------------------------------------------------
+ * Body force and discrete adjoint.  No counterpart in the reference: its
+ * momentum equation has no source term and it computes no derivatives.
+ * ---------------------------------------------------------------------- */
+
+/* Per-cell body force added by the predictor: u* += dt fu, v* += dt fv,
+ * w* += dt fw at the staggered points (i,j,k) of each component.  Each array
+ * is (nx,ny,nz) in Fortran order; a NULL array counts as zero, and three
+ * NULLs remove the force. */
+int ntcfd_set_body_force(ntcfd_ctx* ctx, const double* fu, const double* fv, const double* fw);
+
+typedef struct ntcfd_adj_spec {
+    int nsteps;              /* K: steps taken from the context's current state */
+    int checkpoint_every;    /* M >= 1: (u,v,w,p) kept every M steps, the rest recomputed */
+    double w_drag, w_lift;   /* J = (1/K) sum over the K steps of (w_drag cDrag + w_lift cLift) */
+    double adj_zeta;         /* adjoint Poisson stop rule: max|change| <= adj_zeta * max|rhs| (0: 1e-10) */
+    int adj_itmax;           /* sweep cap of one adjoint Poisson solve (0: 20000) */
+    int inflow_wall;         /* NTCFD_WEST..NTCFD_FRONT, or -1: the wall whose Dirichlet values are */
+    int inflow_normal;       /*   bc_value[inflow_wall][inflow_normal]     = U cos(theta) */
+    int inflow_tangential;   /*   bc_value[inflow_wall][inflow_tangential] = U sin(theta) */
+    int initial_bc;          /* 1: apply boundary_conditions() to the state first (as main.f90:100
+                                does at start-up) and differentiate through it; 0: the state,
+                                ghosts included, is held fixed */
+    int reserved[3];         /* must be zero */
+} ntcfd_adj_spec;
+
+typedef struct ntcfd_adj_result {
+    double J;                /* objective of the forward pass */
+    double dJ_dbc[6][3];     /* dJ / d bc_value[wall][component] (Dirichlet walls; 0 elsewhere) */
+    double dJ_dU;            /* inflow speed and angle (radians) from inflow_wall, else 0 */
+    double dJ_dtheta;
+    double forward_ms;       /* device time of the K steps of the forward pass */
+    double total_ms;         /* wall time of the whole call */
+    long long adj_sweeps;    /* sweeps of all adjoint Poisson solves */
+    int adj_unconverged;     /* adjoint solves that stopped at adj_itmax */
+    int recomputed_steps;    /* forward steps re-run from checkpoints */
+    int fwd_status;          /* status of the forward pass (0 or NTCFD_NOT_CONVERGED) */
+    int pad;
+} ntcfd_adj_result;
+
+/* Discrete adjoint of K steps.  Runs the K steps forward from the current
+ * state (checkpointing every M steps), then the reverse pass: each step's
+ * boundary conditions, force integral, projection and direct forcing,
+ * converged pressure solve (the same SOR kernels on the transposed system),
+ * divergence, QUICK predictor and Smagorinsky nu_t transposed about the
+ * recomputed forward state.  The initial state is held fixed (after the
+ * optional initial boundary conditions, see initial_bc); the pressure
+ * solves are differentiated as exact solves (their initial guess does not
+ * enter), the QUICK upwind branches and the force-integral guards as fixed.
+ * dJ_df* (each (nx,ny,nz), Fortran order, may be NULL) receive dJ/dfu,
+ * dJ/dfv, dJ/dfw of the body force.  per_step (K entries, may be NULL)
+ * receives the forward steps' records.  On return the context holds the
+ * state after the K steps, as ntcfd_step(ctx, K, ...) would leave it. */
+int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_adj_result* result,
+                  double* dJ_dfu, double* dJ_dfv, double* dJ_dfw, ntcfd_step_info* per_step);
+
 #ifdef __cplusplus
 }
 #endif

@@ -77,6 +77,27 @@ class NtcfdKernelTimes(ctypes.Structure):
                                               "resident_sweeps")]
 
 
+class NtcfdAdjSpec(ctypes.Structure):
+    _fields_ = [
+        ("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int),
+        ("w_drag", ctypes.c_double), ("w_lift", ctypes.c_double),
+        ("adj_zeta", ctypes.c_double), ("adj_itmax", ctypes.c_int),
+        ("inflow_wall", ctypes.c_int), ("inflow_normal", ctypes.c_int),
+        ("inflow_tangential", ctypes.c_int), ("initial_bc", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
+    ]
+
+
+class NtcfdAdjResult(ctypes.Structure):
+    _fields_ = [
+        ("J", ctypes.c_double), ("dJ_dbc", (ctypes.c_double * 3) * 6),
+        ("dJ_dU", ctypes.c_double), ("dJ_dtheta", ctypes.c_double),
+        ("forward_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+        ("adj_sweeps", ctypes.c_longlong), ("adj_unconverged", ctypes.c_int),
+        ("recomputed_steps", ctypes.c_int), ("fwd_status", ctypes.c_int), ("pad", ctypes.c_int),
+    ]
+
+
 def f4(x: float) -> float:
     """Value of a Fortran default-real literal stored in a real*8 variable
     (e.g. ``real*8, parameter :: dt = 1.0e-3`` is 0.0010000000474974513)."""
@@ -155,6 +176,10 @@ SIGNATURES = {
     "ntcfd_last_step_ms": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "ntcfd_time_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                           ctypes.POINTER(NtcfdKernelTimes)]),
+    "ntcfd_set_body_force": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 3),
+    "ntcfd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NtcfdAdjSpec),
+                                     ctypes.POINTER(NtcfdAdjResult), _DP, _DP, _DP,
+                                     ctypes.POINTER(NtcfdStepInfo)]),
     # host-side grid generation and geometry (include/ntcfd_host.h)
     "ntcfd_gridder_equal": (None, [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_DP] * 9),
     "ntcfd_gridder_unequal": (None, [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_DP] + [_DP] * 9),

@@ -47,6 +47,8 @@ struct PredArgs {
     double* ws;
     double dt, nu;
     int les;
+    const double* fb;    // body force (fu, fv, fw: three natural-layout arrays, N apart), or null
+    long long fstride;   // N
 };
 
 // One thread per cell (i,j,k), i fastest.  Reads u,v,w (+-2 stencil) and
@@ -91,7 +93,7 @@ __global__ void __launch_bounds__(256) k_predictor(Geom g, Tabs<T> tb, PredArgs 
                   + nue * dt * ((U1 - U0) * X.riD[i + 1] - (U0 - Um1) * X.riD[i]) * X.rDs[i]
                   + nue * dt * ((Un1 - U0) * Y.rDs[j] - (U0 - Us1) * Y.rDs[j - 1]) * Y.riD[j]
                   + nue * dt * ((Uf1 - U0) * Z.rDs[k] - (U0 - Ub1) * Z.rDs[k - 1]) * Z.riD[k];
-        a.us[c] = (double)r;
+        a.us[c] = a.fb ? (double)r + a.dt * __ldg(a.fb + c) : (double)r;
     }
     // ---------------- v* (discretisation_QUICK_centre.f90:127-226)
     {
@@ -116,7 +118,7 @@ __global__ void __launch_bounds__(256) k_predictor(Geom g, Tabs<T> tb, PredArgs 
                   + nue * dt * ((V1 - V0) * X.rDs[i] - (V0 - Vm1) * X.rDs[i - 1]) * X.riD[i]
                   + nue * dt * ((Vn1 - V0) * Y.riD[j + 1] - (V0 - Vs1) * Y.riD[j]) * Y.rDs[j]
                   + nue * dt * ((Vf1 - V0) * Z.rDs[k] - (V0 - Vb1) * Z.rDs[k - 1]) * Z.riD[k];
-        a.vs[c] = (double)r;
+        a.vs[c] = a.fb ? (double)r + a.dt * __ldg(a.fb + a.fstride + c) : (double)r;
     }
     // ---------------- w* (discretisation_QUICK_centre.f90:240-339)
     {
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(256) k_predictor(Geom g, Tabs<T> tb, PredArgs 
                   + nue * dt * ((W1 - W0) * X.rDs[i] - (W0 - Wm1) * X.rDs[i - 1]) * X.riD[i]
                   + nue * dt * ((Wn1 - W0) * Y.rDs[j] - (W0 - Ws1) * Y.rDs[j - 1]) * Y.riD[j]
                   + nue * dt * ((Wf1 - W0) * Z.riD[k + 1] - (W0 - Wb1) * Z.riD[k]) * Z.rDs[k];
-        a.ws[c] = (double)r;
+        a.ws[c] = a.fb ? (double)r + a.dt * __ldg(a.fb + 2 * a.fstride + c) : (double)r;
     }
 #undef LD
 }

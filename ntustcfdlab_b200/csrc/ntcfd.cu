@@ -7,6 +7,7 @@
 // sweeps), so a step needs no host round trip; ntcfd_step(n) launches the
 // graph n times and copies back one small record per step.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -20,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/ntcfd.h"
+#include "k_adjoint.cuh"
 #include "k_mask.cuh"
 #include "k_predictor.cuh"
 #include "k_pressure.cuh"
@@ -55,6 +57,7 @@ struct ntcfd_ctx {
     double *u = nullptr, *v = nullptr, *w = nullptr, *p = nullptr;
     double *us = nullptr, *vs = nullptr, *ws = nullptr, *b = nullptr;
     double *eta = nullptr, *nut = nullptr;
+    double* fb = nullptr;                   // body force fu, fv, fw (3 natural arrays), null when unset
     void *eR = nullptr, *eB = nullptr, *dR = nullptr, *dB = nullptr;
     void *rdR = nullptr, *rdB = nullptr;   // 1/diag per colour (sweep precision)
     double* tabd = nullptr;   // double tables
@@ -284,7 +287,7 @@ int build_graph(ntcfd_ctx* ctx) {
         dep = {n};
     }
     PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
-                P.dt, 1. / P.Re, P.LES};
+                P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
     GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
     dep = {n};
     GK(add_kernel(&n, G, dep, k_rhs, g3, b3, g, ctx->scd, (const double*)ctx->u,
@@ -393,6 +396,70 @@ int build_graph(ntcfd_ctx* ctx) {
     return 0;
 }
 
+// One SOR solve launched from the host: the graph's loop structure (defect-
+// correction cycles around the resident kernel or around streaming sweeps
+// with a stop test every check_every sweeps), on pressure `p` (interior
+// updated, ghosts read) with right-hand side `b`, stop rule max|change| <=
+// zeta and sweep cap itmax.  *hc receives the final control block.
+template <class Tc>
+int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int itmax, Ctl* hc) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaStream_t st = ctx->stream;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+    const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
+    k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
+    Ctl& h = *hc;
+    h = Ctl{};
+    auto read_ctl = [&]() -> int {
+        CK(cudaMemcpyAsync(&h, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return 0;
+    };
+    bool more = itmax > 0;
+    const int big_guard = ctx->csweeps > 1 ? 1 : 0;
+    while (more) {
+        if (ctx->resident) {
+            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, ctx->ring,
+                                            (unsigned int*)ctx->bar);
+            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&eR,
+                            (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
+                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&zeta,
+                            (void*)&itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
+            CK(cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
+                                           dim3(kResNT), args, ctx->res_smem, st));
+        } else {
+            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, nullptr,
+                                            nullptr);
+            const dim3 bs(kSweepBx, kSweepBy, 1);
+            const int half = (g.nx + 1) / 2;
+            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
+                          (g.nz + kSweepKpt - 1) / kSweepKpt);
+            for (;;) {
+                for (int sub = 0; sub < ctx->csweeps; ++sub) {
+                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, sub, itmax,
+                        ctx->cycle_len, big_guard, ctx->slots);
+                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, sub, itmax,
+                        ctx->cycle_len, big_guard, ctx->slots);
+                }
+                k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
+                                              zeta, 0, 0);
+                if (int rc = read_ctl()) return rc;
+                if (h.pad_stop) break;
+            }
+            k_correct<Tc><<<g3, b3, 0, st>>>(g, p, eR, eB);
+        }
+        k_outer_check<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
+        if (int rc = read_ctl()) return rc;
+        more = h.pad_more != 0;
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
 // One step with every kernel launched from the host (no CUDA graph): the
 // same kernels and loop decisions as the graph, for kernel profilers (which
 // cannot look inside graphs that contain conditional nodes) and debugging.
@@ -402,61 +469,15 @@ int run_step_eager(ntcfd_ctx* ctx) {
     const ntcfd_params& P = ctx->prm;
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
-    Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
-    const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
     if (P.LES)
         k_smagorinsky<<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
                                          P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
     PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
-                P.dt, 1. / P.Re, P.LES};
+                P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
     k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
     k_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
-    k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
     Ctl h{};
-    auto read_ctl = [&]() -> int {
-        CK(cudaMemcpyAsync(&h, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        return 0;
-    };
-    bool more = P.itmax > 0;
-    const int big_guard = ctx->csweeps > 1 ? 1 : 0;
-    while (more) {
-        if (ctx->resident) {
-            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB, ctx->ctl, 0, 0,
-                                            ctx->ring, (unsigned int*)ctx->bar);
-            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&ctx->p, (void*)&eR,
-                            (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
-                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&P.zeta,
-                            (void*)&P.itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
-            CK(cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
-                                           dim3(kResNT), args, ctx->res_smem, st));
-        } else {
-            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB, ctx->ctl, 0, 0,
-                                            nullptr, nullptr);
-            const dim3 bs(kSweepBx, kSweepBy, 1);
-            const int half = (g.nx + 1) / 2;
-            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
-                          (g.nz + kSweepKpt - 1) / kSweepKpt);
-            for (;;) {
-                for (int sub = 0; sub < ctx->csweeps; ++sub) {
-                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
-                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, sub, P.itmax,
-                        ctx->cycle_len, big_guard, ctx->slots);
-                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
-                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, sub, P.itmax,
-                        ctx->cycle_len, big_guard, ctx->slots);
-                }
-                k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, P.itmax, ctx->cycle_len,
-                                              P.zeta, 0, 0);
-                if (int rc = read_ctl()) return rc;
-                if (h.pad_stop) break;
-            }
-            k_correct<Tc><<<g3, b3, 0, st>>>(g, ctx->p, eR, eB);
-        }
-        k_outer_check<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
-        if (int rc = read_ctl()) return rc;
-        more = h.pad_more != 0;
-    }
+    if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, &h)) return rc;
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
     k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0, st>>>(g, pj);
@@ -567,7 +588,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     };
     int rc;
     PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
-                P.dt, 1. / P.Re, P.LES};
+                P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
     if ((rc = timed([&] {
              if (P.LES)
                  k_smagorinsky<<<g3, b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
@@ -963,14 +984,16 @@ int ntcfd_get_output(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double
     return 0;
 }
 
-int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
-    DEV();
-    if (nsteps < 0) return fail(ctx, NTCFD_EINVAL, "nsteps < 0");
-    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_step");
-    if (nsteps == 0) return 0;
-    if (nsteps > ctx->rec_cap) {
+}  // extern "C"
+
+namespace {
+
+// Record buffer of at least nrec steps and an instantiated step graph (the
+// graph is built in eager mode too: it plans the SOR path).
+int prepare_steps(ntcfd_ctx* ctx, int nrec) {
+    if (nrec > ctx->rec_cap) {
         // the graph holds the record pointer: grow the record buffer, then rebuild
-        const int cap = std::max(nsteps, 1024);
+        const int cap = std::max(nrec, 1024);
         if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
         if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
         if (ctx->rec) cudaFree(ctx->rec);
@@ -980,26 +1003,23 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
         ctx->rec_cap = cap;
     }
     if (!ctx->exec) {
-        // the graph is built in eager mode too: it plans the SOR path
         const int rc = ctx->prm.precision == NTCFD_MIXED ? build_graph<float>(ctx) : build_graph<double>(ctx);
         if (rc) return rc;
     }
-    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (int s = 0; s < nsteps; ++s) {
-        if (ctx->prm.eager) {
-            const int rc = ctx->prm.precision == NTCFD_MIXED ? run_step_eager<float>(ctx)
-                                                             : run_step_eager<double>(ctx);
-            if (rc) return rc;
-        } else {
-            CK(cudaGraphLaunch(ctx->exec, ctx->stream));
-        }
-    }
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    std::vector<StepRec> rec(nsteps);
-    CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    return 0;
+}
+
+// One step on the context's stream; its record goes to rec[ctl->step].
+int launch_step(ntcfd_ctx* ctx) {
+    if (ctx->prm.eager)
+        return ctx->prm.precision == NTCFD_MIXED ? run_step_eager<float>(ctx) : run_step_eager<double>(ctx);
+    CK(cudaGraphLaunch(ctx->exec, ctx->stream));
+    return 0;
+}
+
+// Advances the simulated time by one dt per record, fills `info` (may be
+// NULL) and returns the worst status of the records.
+int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_info* info) {
     int status = 0;
     for (int s = 0; s < nsteps; ++s) {
         ctx->time = ctx->time + ctx->prm.dt;   // main.f90:271
@@ -1024,6 +1044,28 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     else if (status == NTCFD_ENONFINITE) fail(ctx, status, "non-finite value in the SOR solve");
     else if (status == NTCFD_NOT_CONVERGED) fail(ctx, status, "SOR stopped at itmax in at least one step");
     return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
+    DEV();
+    if (nsteps < 0) return fail(ctx, NTCFD_EINVAL, "nsteps < 0");
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_step");
+    if (nsteps == 0) return 0;
+    if (int rc = prepare_steps(ctx, nsteps)) return rc;
+    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int s = 0; s < nsteps; ++s)
+        if (int rc = launch_step(ctx)) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    std::vector<StepRec> rec(nsteps);
+    CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    return records_to_info(ctx, rec.data(), nsteps, info);
 }
 
 int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms) {
@@ -1257,4 +1299,332 @@ extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az
         return fail(ctx, NTCFD_EINVAL,
                     "%d exact vertex/grid ties: the reference resolves them by moving the grid", hties);
     return 0;
+}
+
+// ============================================================ body force
+extern "C" int ntcfd_set_body_force(ntcfd_ctx* ctx, const double* fu, const double* fv, const double* fw) {
+    DEV();
+    const Geom& g = ctx->g;
+    const size_t N = ctx->nat_elems;
+    if (!fu && !fv && !fw) {
+        if (ctx->fb) {
+            // the graph holds the pointer: drop it so that the next step rebuilds without the force
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+            if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+            ctx->fb = nullptr;   // the storage stays in ctx->allocs
+        }
+        return 0;
+    }
+    if (!ctx->fb) {
+        double* q = nullptr;
+        if (int rc = dalloc(ctx, &q, 3 * N)) return rc;
+        ctx->fb = q;
+        if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    }
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    const double* src[3] = {fu, fv, fw};
+    const dim3 b3(32, 4, 2);
+    for (int c = 0; c < 3; ++c) {
+        double* dst = ctx->fb + c * N;
+        if (!src[c]) {
+            CK(cudaMemsetAsync(dst, 0, N * sizeof(double), ctx->stream));
+            continue;
+        }
+        for (size_t q = 0; q < n; ++q)
+            if (!std::isfinite(src[c][q])) return fail(ctx, NTCFD_EINVAL, "non-finite body force");
+        CK(cudaMemcpyAsync(ctx->outbuf, src[c], n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        k_interior_in<<<grid3(g, b3), b3, 0, ctx->stream>>>(g, ctx->outbuf, dst);
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// ============================================================ adjoint
+namespace {
+
+// Device storage of one ntcfd_adjoint call, released on every return path.
+struct AdjMem {
+    std::vector<void*> blocks;
+    ~AdjMem() {
+        for (void* q : blocks) cudaFree(q);
+    }
+    template <class T>
+    cudaError_t get(T** out, size_t n) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 256);
+        if (e != cudaSuccess) return e;
+        blocks.push_back(q);
+        *out = reinterpret_cast<T*>(q);
+        return cudaSuccess;
+    }
+};
+
+struct AdjBufs {
+    double *lu, *lv, *lw, *lp, *lpn, *lus, *lvs, *lws, *z, *badj, *lb, *wD, *wL, *lnut, *gf, *gval;
+    unsigned long long* slot;
+};
+
+// Reverse of one step: on entry lu, lv, lw, lp hold the adjoint of the state
+// after the step; on return the adjoint of the state before it.  (su, sv, sw)
+// is the velocity before the step, `guards` the step's force-integral guards.
+template <class Tc>
+int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv, const double* sw,
+                 const unsigned char* guards, double scaleD, double scaleL, double zeta_rel, int itmax,
+                 long long* sweeps, int* unconverged) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaStream_t st = ctx->stream;
+    const size_t N = ctx->nat_elems;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    const dim3 b3s(32, 2, 2), g3s = grid3(g, b3s);   // 128-thread blocks
+    CK(cudaMemsetAsync(A.lpn, 0, N * sizeof(double), st));
+    AdjBcArgs ab{};
+    ab.lu = A.lu; ab.lv = A.lv; ab.lw = A.lw; ab.lp = A.lp;
+    std::memcpy(ab.bc, P.bc, sizeof ab.bc);
+    ab.gval = A.gval;
+    k_adj_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ab);
+    k_adj_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ab);
+    k_adj_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ab);
+    k_adj_weights<<<g3, b3, 0, st>>>(g, guards, scaleD, scaleL, A.wD, A.wL);
+    k_adj_project1<<<g3, b3, 0, st>>>(g, A.lu, A.lv, A.lw, ctx->eta, A.wD, A.wL, P.dt, A.lus, A.lvs, A.lws);
+    k_adj_project2<<<g3, b3, 0, st>>>(g, A.lus, A.lvs, A.lws, P.dt, A.lp, A.lpn);
+    k_adj_solve_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, A.lp, A.badj);
+    CK(cudaMemsetAsync(A.slot, 0, sizeof(unsigned long long), st));
+    k_absmax<256><<<g3, b3, 0, st>>>(g, A.badj, A.slot);
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, A.slot, sizeof bits, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaGetLastError());
+    double bmax;
+    std::memcpy(&bmax, &bits, sizeof bmax);
+    if (!std::isfinite(bmax)) return fail(ctx, NTCFD_ENONFINITE, "non-finite adjoint pressure right-hand side");
+    if (bmax > 0.0) {
+        Ctl h{};
+        if (int rc = sor_solve_eager<Tc>(ctx, A.z, A.badj, zeta_rel * bmax, itmax, &h)) return rc;
+        if (h.timeout) return fail(ctx, NTCFD_ETIMEOUT, "the resident SOR kernel's grid barrier gave up waiting");
+        if (h.nonfinite) return fail(ctx, NTCFD_ENONFINITE, "non-finite value in an adjoint SOR solve");
+        *sweeps += h.ik;
+        if (!h.converged) *unconverged += 1;
+    } else {
+        CK(cudaMemsetAsync(A.z, 0, N * sizeof(double), st));
+    }
+    k_adj_after_solve<<<g3, b3, 0, st>>>(g, ctx->scd, A.z, A.lb, A.lpn);
+    k_adj_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, A.lb, P.dt, A.lus, A.lvs, A.lws, A.lu, A.lv, A.lw);
+    const int aliased = P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0;
+    if (P.LES) {
+        k_smagorinsky<<<g3, b3, 0, st>>>(g, su, sv, sw, ctx->nut, P.Cs, aliased);
+        CK(cudaMemsetAsync(A.lnut, 0, N * sizeof(double), st));
+    }
+    AdjPredArgs pa{su, sv, sw, P.LES ? ctx->nut : nullptr, A.lus, A.lvs, A.lws, A.lu, A.lv, A.lw,
+                   P.LES ? A.lnut : nullptr, A.gf, (long long)N, P.dt, 1. / P.Re, P.LES};
+    k_adj_predictor<<<g3s, b3s, 0, st>>>(g, ctx->tpd, pa);
+    if (P.LES)
+        k_adj_smagorinsky<<<g3s, b3s, 0, st>>>(g, su, sv, sw, A.lnut, P.Cs, aliased, A.lu, A.lv, A.lw);
+    CK(cudaGetLastError());
+    std::swap(A.lp, A.lpn);
+    return 0;
+}
+
+template <class Tc>
+int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, double* gout[3],
+              ntcfd_step_info* per_step) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaStream_t st = ctx->stream;
+    const size_t N = ctx->nat_elems;
+    const int K = sp->nsteps, M = sp->checkpoint_every;
+    const int nck = (K + M - 1) / M;
+    const size_t G = 2 * (size_t)g.nx * g.ny + 2 * (size_t)g.nx;   // guard bytes per step
+    const size_t fyz = (size_t)g.ny * g.nz, fxz = (size_t)g.nx * g.nz, fxy = (size_t)g.nx * g.ny;
+    const size_t nface = 2 * (fyz + fxz + fxy);
+    AdjMem mem;
+    double *ckpt, *blk, *fin;
+    unsigned char* guards;
+    AdjBufs A{};
+    CK(mem.get(&ckpt, (size_t)nck * 4 * N));
+    CK(mem.get(&blk, (size_t)M * 3 * N));
+    CK(mem.get(&fin, 4 * N + nface));
+    CK(mem.get(&guards, (size_t)K * G));
+    double** lam[] = {&A.lu, &A.lv, &A.lw, &A.lp, &A.lpn, &A.lus, &A.lvs, &A.lws, &A.z, &A.badj, &A.lb,
+                      &A.wD, &A.wL};
+    for (double** q : lam) {
+        CK(mem.get(q, N));
+        CK(cudaMemsetAsync(*q, 0, N * sizeof(double), st));
+    }
+    if (P.LES) CK(mem.get(&A.lnut, N));
+    CK(mem.get(&A.gf, 3 * N));
+    CK(cudaMemsetAsync(A.gf, 0, 3 * N * sizeof(double), st));
+    CK(mem.get(&A.gval, 18));
+    CK(cudaMemsetAsync(A.gval, 0, 18 * sizeof(double), st));
+    CK(mem.get(&A.slot, 1));
+    if (int rc = prepare_steps(ctx, std::max(K, M))) return rc;
+    auto save_state = [&](double* dst) -> int {
+        double* src[4] = {ctx->u, ctx->v, ctx->w, ctx->p};
+        for (int q = 0; q < 4; ++q)
+            CK(cudaMemcpyAsync(dst + q * N, src[q], N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return 0;
+    };
+    auto load_state = [&](const double* srcb) -> int {
+        double* dst[4] = {ctx->u, ctx->v, ctx->w, ctx->p};
+        for (int q = 0; q < 4; ++q)
+            CK(cudaMemcpyAsync(dst[q], srcb + q * N, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        return 0;
+    };
+    double* faces[6] = {ctx->faceW, ctx->faceE, ctx->faceS, ctx->faceN, ctx->faceB, ctx->faceF};
+    const size_t flen[6] = {fyz, fyz, fxz, fxz, fxy, fxy};
+    BcArgs ba{};
+    ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+    std::memcpy(ba.bc, P.bc, sizeof ba.bc);
+    std::memcpy(ba.val, P.bc_value, sizeof ba.val);
+    ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
+    ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
+    const dim3 gbx((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), gby((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8),
+        gbz((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), bbc(32, 8);
+    if (sp->initial_bc) {
+        k_bc_x<<<gbx, bbc, 0, st>>>(g, ba);
+        k_bc_y<<<gby, bbc, 0, st>>>(g, ba);
+        k_bc_z<<<gbz, bbc, 0, st>>>(g, ba);
+        CK(cudaGetLastError());
+    }
+    // ---- forward pass: K steps, a checkpoint every M, the guards of every step
+    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), st));
+    CK(cudaEventRecord(ctx->ev0, st));
+    for (int s = 0; s < K; ++s) {
+        if (s % M == 0)
+            if (int rc = save_state(ckpt + (size_t)(s / M) * 4 * N)) return rc;
+        if (int rc = launch_step(ctx)) return rc;
+        k_pack_guards<<<148, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, guards + (size_t)s * G);
+    }
+    CK(cudaEventRecord(ctx->ev1, st));
+    CK(cudaGetLastError());
+    std::vector<StepRec> rec(K);
+    CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * K, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float fms = 0.0f;
+    CK(cudaEventElapsedTime(&fms, ctx->ev0, ctx->ev1));
+    res->forward_ms = fms;
+    const int fst = records_to_info(ctx, rec.data(), K, per_step);
+    if (fst < 0) return fst;
+    res->fwd_status = fst;
+    double J = 0.0;
+    for (int s = 0; s < K; ++s) J += sp->w_drag * rec[s].cdrag + sp->w_lift * rec[s].clift;
+    res->J = J / K;
+    if (int rc = save_state(fin)) return rc;
+    {
+        size_t off = 4 * N;
+        for (int q = 0; q < 6; ++q) {
+            CK(cudaMemcpyAsync(fin + off, faces[q], flen[q] * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            off += flen[q];
+        }
+    }
+    // ---- reverse pass, block by block from the last checkpoint
+    const double scaleD = sp->w_drag * (-2.0 / P.lx) / K;
+    const double scaleL = sp->w_lift * (-2.0 / P.lx) / K;
+    const double zrel = sp->adj_zeta > 0 ? sp->adj_zeta : 1e-10;
+    const int itmax = sp->adj_itmax > 0 ? sp->adj_itmax : 20000;
+    long long sweeps = 0;
+    int unconv = 0, recomputed = 0;
+    for (int b = nck - 1; b >= 0; --b) {
+        const int s0 = b * M, s1 = std::min(K, s0 + M);
+        if (int rc = load_state(ckpt + (size_t)b * 4 * N)) return rc;
+        CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), st));
+        for (int m = 0; m < s1 - s0; ++m) {
+            double* dst = blk + (size_t)m * 3 * N;
+            CK(cudaMemcpyAsync(dst, ctx->u, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(dst + N, ctx->v, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(dst + 2 * N, ctx->w, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if (m + 1 < s1 - s0) {
+                if (int rc = launch_step(ctx)) return rc;
+                ++recomputed;
+            }
+        }
+        for (int n = s1 - 1; n >= s0; --n) {
+            const double* sb = blk + (size_t)(n - s0) * 3 * N;
+            if (int rc = adjoint_step<Tc>(ctx, A, sb, sb + N, sb + 2 * N, guards + (size_t)n * G, scaleD, scaleL,
+                                          zrel, itmax, &sweeps, &unconv))
+                return rc;
+        }
+    }
+    if (sp->initial_bc) {
+        // the initial boundary conditions, transposed (lam of the state before them is not kept)
+        AdjBcArgs ab{};
+        ab.lu = A.lu; ab.lv = A.lv; ab.lw = A.lw; ab.lp = A.lp;
+        std::memcpy(ab.bc, P.bc, sizeof ab.bc);
+        ab.gval = A.gval;
+        k_adj_bc_z<<<gbz, bbc, 0, st>>>(g, ab);
+        k_adj_bc_y<<<gby, bbc, 0, st>>>(g, ab);
+        k_adj_bc_x<<<gbx, bbc, 0, st>>>(g, ab);
+        CK(cudaGetLastError());
+    }
+    // ---- results
+    double gv[18];
+    CK(cudaMemcpyAsync(gv, A.gval, sizeof gv, cudaMemcpyDeviceToHost, st));
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    const dim3 b3(32, 4, 2);
+    for (int c = 0; c < 3; ++c) {
+        if (!gout[c]) continue;
+        k_interior_out<<<grid3(g, b3), b3, 0, st>>>(g, A.gf + c * N, ctx->outbuf);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(gout[c], ctx->outbuf, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    // the state after the K steps, as the forward pass left it
+    if (int rc = load_state(fin)) return rc;
+    {
+        size_t off = 4 * N;
+        for (int q = 0; q < 6; ++q) {
+            CK(cudaMemcpyAsync(faces[q], fin + off, flen[q] * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            off += flen[q];
+        }
+    }
+    CK(cudaStreamSynchronize(st));
+    for (int q = 0; q < 18; ++q) res->dJ_dbc[q / 3][q % 3] = gv[q];
+    if (sp->inflow_wall >= 0) {
+        const double* val = P.bc_value[sp->inflow_wall];
+        const double a = val[sp->inflow_normal], t = val[sp->inflow_tangential];
+        const double U = std::hypot(a, t), th = std::atan2(t, a);
+        const double ga = gv[sp->inflow_wall * 3 + sp->inflow_normal];
+        const double gt = gv[sp->inflow_wall * 3 + sp->inflow_tangential];
+        res->dJ_dU = ga * std::cos(th) + gt * std::sin(th);
+        res->dJ_dtheta = U * (-ga * std::sin(th) + gt * std::cos(th));
+    }
+    res->adj_sweeps = sweeps;
+    res->adj_unconverged = unconv;
+    res->recomputed_steps = recomputed;
+    res->total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return unconv ? NTCFD_NOT_CONVERGED : fst;
+}
+
+}  // namespace
+
+extern "C" int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_adj_result* result,
+                             double* dJ_dfu, double* dJ_dfv, double* dJ_dfw, ntcfd_step_info* per_step) {
+    DEV();
+    if (!spec || !result) return fail(ctx, NTCFD_EINVAL, "null spec or result");
+    std::memset(result, 0, sizeof *result);
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_adjoint");
+    if (spec->nsteps < 1) return fail(ctx, NTCFD_EINVAL, "nsteps must be >= 1");
+    if (spec->checkpoint_every < 1) return fail(ctx, NTCFD_EINVAL, "checkpoint_every must be >= 1");
+    if (!(spec->adj_zeta >= 0.0) || spec->adj_itmax < 0) return fail(ctx, NTCFD_EINVAL, "bad adjoint stop rule");
+    if (!std::isfinite(spec->w_drag) || !std::isfinite(spec->w_lift))
+        return fail(ctx, NTCFD_EINVAL, "non-finite objective weights");
+    if (spec->initial_bc != 0 && spec->initial_bc != 1) return fail(ctx, NTCFD_EINVAL, "initial_bc must be 0 or 1");
+    for (int r : spec->reserved)
+        if (r) return fail(ctx, NTCFD_EINVAL, "reserved fields of ntcfd_adj_spec must be zero");
+    if (spec->inflow_wall < -1 || spec->inflow_wall > 5)
+        return fail(ctx, NTCFD_EINVAL, "inflow_wall must be -1 or a wall index");
+    if (spec->inflow_wall >= 0 &&
+        (spec->inflow_normal < 0 || spec->inflow_normal > 2 || spec->inflow_tangential < 0 ||
+         spec->inflow_tangential > 2 || spec->inflow_normal == spec->inflow_tangential))
+        return fail(ctx, NTCFD_EINVAL, "inflow components must be two distinct indices in 0..2");
+    double* gout[3] = {dJ_dfu, dJ_dfv, dJ_dfw};
+    const int rc = ctx->prm.precision == NTCFD_MIXED ? adjoint_t<float>(ctx, spec, result, gout, per_step)
+                                                     : adjoint_t<double>(ctx, spec, result, gout, per_step);
+    if (rc == NTCFD_NOT_CONVERGED && result->adj_unconverged)
+        fail(ctx, rc, "%d adjoint pressure solves stopped at adj_itmax", result->adj_unconverged);
+    return rc;
 }

@@ -205,3 +205,59 @@ class Solver:
         self._check(self.lib.ntcfd_time_kernels(self.h, reps, ctypes.byref(t)))
         return {n: getattr(t, n) for n in ("predictor_ms", "rhs_ms", "defect_ms", "sweep_ms",
                                            "project_ms", "bc_ms", "resident_ms", "resident_sweeps")}
+
+    # ------------------------------------------------------------ adjoint
+    def set_body_force(self, fu=None, fv=None, fw=None):
+        """Per-cell body force on the u, v, w momentum (each (nx, ny, nz) or None = 0)."""
+        arrs = []
+        for f in (fu, fv, fw):
+            if f is None:
+                arrs.append(None)
+                continue
+            a = np.asfortranarray(f, dtype=np.float64)
+            if a.shape != self.inner_shape:
+                raise ValueError(f"body force arrays must have shape {self.inner_shape}")
+            arrs.append(a)
+        ptrs = [dptr(a) if a is not None else None for a in arrs]
+        self._check(self.lib.ntcfd_set_body_force(self.h, *ptrs))
+
+    def adjoint(self, nsteps: int, checkpoint_every: int, *, w_drag: float = 1.0,
+                w_lift: float = 0.0, adj_zeta: float = 0.0, adj_itmax: int = 0,
+                inflow=None, force_grad: bool = True, initial_bc: bool = False) -> dict:
+        """Discrete adjoint of `nsteps` steps from the current state (ntcfd_adjoint).
+
+        J = mean over the steps of (w_drag cDrag + w_lift cLift).  `inflow` =
+        (wall, normal component, tangential component) names the Dirichlet
+        values that hold U cos(theta), U sin(theta).  initial_bc applies the
+        boundary conditions to the state first and differentiates through
+        them (otherwise the state, ghosts included, is fixed).  Returns a dict with J,
+        dJ_dbc (6x3), dJ_dU, dJ_dtheta, dJ_df (3 arrays or None), the step
+        records and the timings; the solver is left after the nsteps steps."""
+        spec = abi.NtcfdAdjSpec()
+        spec.nsteps, spec.checkpoint_every = nsteps, checkpoint_every
+        spec.w_drag, spec.w_lift = w_drag, w_lift
+        spec.adj_zeta, spec.adj_itmax = adj_zeta, adj_itmax
+        spec.initial_bc = 1 if initial_bc else 0
+        if inflow is None:
+            spec.inflow_wall, spec.inflow_normal, spec.inflow_tangential = -1, 0, 1
+        else:
+            wall, cn, ct = inflow
+            spec.inflow_wall = abi.WALL_NAMES.index(wall) if isinstance(wall, str) else wall
+            spec.inflow_normal, spec.inflow_tangential = cn, ct
+        res = abi.NtcfdAdjResult()
+        grads = [np.zeros(self.inner_shape, dtype=np.float64, order="F") for _ in range(3)] \
+            if force_grad else [None] * 3
+        info = (NtcfdStepInfo * nsteps)()
+        rc = self.lib.ntcfd_adjoint(self.h, ctypes.byref(spec), ctypes.byref(res),
+                                    *[dptr(a) if a is not None else None for a in grads], info)
+        self._check(rc, allow_warning=True)
+        return {
+            "J": res.J,
+            "dJ_dbc": np.array([[res.dJ_dbc[w][c] for c in range(3)] for w in range(6)]),
+            "dJ_dU": res.dJ_dU, "dJ_dtheta": res.dJ_dtheta,
+            "dJ_df": grads if force_grad else None,
+            "forward_ms": res.forward_ms, "total_ms": res.total_ms,
+            "adj_sweeps": res.adj_sweeps, "adj_unconverged": res.adj_unconverged,
+            "recomputed_steps": res.recomputed_steps, "status": rc,
+            "info": list(info),
+        }
