@@ -17,6 +17,12 @@ across GPUs); value = total cells * steps / max-over-ranks device time.
 --impl reference times the CPU restatement of the reference's own algorithm
 (lexicographic SOR with the reference's OpenMP loop schedule) on the host
 cores, rank 0 only.
+
+The "adjoint" object (rank 0, one GPU) gives the second half of the metric:
+wall time of ntcfd_adjoint over K = 200 steps of the cylinder case (32x96x96,
+checkpoints every 20 steps) divided by the device time of the plain K-step
+forward, and the agreement of its gradients (inflow speed, inflow angle, a
+random direction of the body force) with central differences.
 """
 from __future__ import annotations
 
@@ -54,6 +60,8 @@ def parse():
                     help="launch kernels one by one instead of CUDA graphs (for ncu)")
     ap.add_argument("--sor-path", choices=("auto", "streaming", "resident"), default="auto")
     ap.add_argument("--no-roofline", action="store_true", help="skip the standalone kernel timing")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost/accuracy leg")
+    ap.add_argument("--no-fd", action="store_true", help="skip the finite-difference check of the adjoint")
     return ap.parse_args()
 
 
@@ -286,6 +294,90 @@ def roofline(s, case, path, reps=20):
             "kernel_ms": {k: round(v, 5) for k, v in kt.items()}}
 
 
+def adjoint_leg(device, fd=True, K=200, M=20):
+    """Adjoint cost and accuracy on the cylinder case: J = mean cDrag over
+    K steps from an impulsive start with the seeded body force, checkpoints
+    every M steps.  Cost = wall time of ntcfd_adjoint / device time of the
+    plain K-step forward (reference zeta 1e-4).  Accuracy = the adjoint
+    (default adjoint stop rule) against central differences h = 1e-6 of
+    K-step runs whose pressure solves run to zeta = 1e-12."""
+    import math
+    from ntustcfdlab_b200 import abi, cases
+    from ntustcfdlab_b200.solver import Solver
+
+    def case(prec, zeta=abi.f4(1e-4), U=1.0, theta_deg=0.0):
+        kw = dict(zeta=zeta, itmax=200000 if zeta < 1e-6 else 3000, device=device)
+        if prec == abi.MIXED:
+            kw["mixed_cycle"] = 8
+        return cases.c4(precision=prec, U=U, theta_deg=theta_deg, **kw)
+
+    base = case(abi.FP64)
+    nx, ny, nz = base.params.nx, base.params.ny, base.params.nz
+    force = cases.body_force_c4((nx, ny, nz))
+    s0 = Solver(base.params, base.grid)
+    s0.set_state(*cases.uniform_inflow_state(base))
+    s0.boundary_conditions()
+    st = s0.get_state()
+    s0.close()
+
+    def solver(c, f=force):
+        s = Solver(c.params, c.grid)
+        s.build_mask_cylinder(c.mask["zc"], c.mask["yc"], c.mask["r"])
+        s.set_state(*st)
+        s.set_body_force(*f)
+        return s
+
+    out = {"case": "cylinder D=1, 32x96x96 (span x, y, z) uniform over 4x12x12, Re=100, dt=5e-3, "
+                   "impulsive start, inflow w=1 on the Back wall, body force N(0,1e-3) seed "
+                   f"{cases.C4_SEED}", "K": K, "M": M, "objective": "mean cDrag over the K steps",
+           "adj_zeta": 1e-7, "adj_omega": 1.9}
+    for prec, name in ((abi.MIXED, "mixed"), (abi.FP64, "fp64")):
+        c = case(prec)
+        s = solver(c)
+        s.step(2)                          # graph instantiation
+        s.set_state(*st)
+        s.adjoint(K, M, w_drag=1.0, inflow=("Back", 2, 1))   # warm-up: workspace, kernel loading
+        s.set_state(*st)
+        info, rc = s.step(K)
+        fwd = s.last_step_ms()
+        s.set_state(*st)
+        r = s.adjoint(K, M, w_drag=1.0, inflow=("Back", 2, 1))
+        s.close()
+        out[name] = {"forward_ms": round(fwd, 3), "adjoint_total_ms": round(r["total_ms"], 3),
+                     "adjoint_over_forward": round(r["total_ms"] / fwd, 3),
+                     "phases_ms": {"forward_pass": round(r["forward_ms"], 3),
+                                   "recompute": round(r["recompute_ms"], 3),
+                                   "adjoint_solves": round(r["solve_ms"], 3)},
+                     "adjoint_sweeps": r["adj_sweeps"], "forward_sweeps": int(sum(i.sor_iters for i in info)),
+                     "dJ_dU": r["dJ_dU"], "dJ_dtheta": r["dJ_dtheta"]}
+    if fd:
+        h = 1e-6
+        tight = case(abi.FP64, zeta=1e-12)
+        s = solver(tight)
+        r = s.adjoint(K, M, w_drag=1.0, inflow=("Back", 2, 1))
+        s.close()
+
+        def J(U=1.0, th=0.0, f=force):
+            s = solver(case(abi.FP64, zeta=1e-12, U=U, theta_deg=math.degrees(th)), f)
+            info, rc = s.step(K)
+            s.close()
+            return sum(i.cDrag for i in info) / K
+
+        gU = (J(U=1 + h) - J(U=1 - h)) / (2 * h)
+        gth = (J(th=h) - J(th=-h)) / (2 * h)
+        rng = np.random.default_rng(11)
+        d = [rng.standard_normal(f.shape) for f in force]
+        gf = (J(f=[a + h * e for a, e in zip(force, d)]) - J(f=[a - h * e for a, e in zip(force, d)])) / (2 * h)
+        ga = sum(float(np.sum(a * e)) for a, e in zip(r["dJ_df"], d))
+        out["fd_check"] = {"forward_zeta": 1e-12, "h": h,
+                           "dJ_dU": [r["dJ_dU"], gU], "dJ_dtheta": [r["dJ_dtheta"], gth],
+                           "dJ_df_dir": [ga, gf],
+                           "rel_err": {"U": abs(r["dJ_dU"] - gU) / abs(gU),
+                                       "theta": abs(r["dJ_dtheta"] - gth) / abs(gth),
+                                       "force_dir": abs(ga - gf) / abs(gf)}}
+    return out
+
+
 def rel_l2(a, b):
     a = a[2:-2, 2:-2, 2:-2]
     b = b[2:-2, 2:-2, 2:-2]
@@ -339,6 +431,9 @@ def run_ours(args):
                "sample": (f"{nst} consecutive steps ({nsw} SOR sweeps, {el:.1f} s) of the same "
                           f"{args.n}^3 case from the device state after step {K}; lexicographic "
                           f"SOR with the reference's OpenMP schedule, {thr} threads")}
+    adj = None
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        adj = adjoint_leg(local, fd=not args.no_fd)
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
@@ -357,7 +452,8 @@ def run_ours(args):
             "sor_sweeps_total": int(sum(sweeps)), "sor_sweeps_per_step": float(np.mean(sweeps)),
             "all_converged": bool(all(i.converged for i in info)),
             "gpu_launches": launches * world,
-            "adjoint_over_forward": None,
+            "adjoint_over_forward": adj["mixed"]["adjoint_over_forward"] if adj else None,
+            "adjoint": adj,
             "roofline": rl, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         }
         line.update(extra)

@@ -218,7 +218,10 @@ typedef struct ntcfd_adj_spec {
     int nsteps;              /* K: steps taken from the context's current state */
     int checkpoint_every;    /* M >= 1: (u,v,w,p) kept every M steps, the rest recomputed */
     double w_drag, w_lift;   /* J = (1/K) sum over the K steps of (w_drag cDrag + w_lift cLift) */
-    double adj_zeta;         /* adjoint Poisson stop rule: max|change| <= adj_zeta * max|rhs| (0: 1e-10) */
+    double adj_zeta;         /* adjoint Poisson stop rule: max|change| <= adj_zeta * max|rhs| (0: 1e-7) */
+    double adj_omega;        /* SOR relaxation of the adjoint solves, 0 < adj_omega < 2 (0: 1.9; the
+                                forward keeps the reference's omega, the adjoint solve is free to
+                                relax closer to the optimum) */
     int adj_itmax;           /* sweep cap of one adjoint Poisson solve (0: 20000) */
     int inflow_wall;         /* NTCFD_WEST..NTCFD_FRONT, or -1: the wall whose Dirichlet values are */
     int inflow_normal;       /*   bc_value[inflow_wall][inflow_normal]     = U cos(theta) */
@@ -234,8 +237,10 @@ typedef struct ntcfd_adj_result {
     double dJ_dbc[6][3];     /* dJ / d bc_value[wall][component] (Dirichlet walls; 0 elsewhere) */
     double dJ_dU;            /* inflow speed and angle (radians) from inflow_wall, else 0 */
     double dJ_dtheta;
-    double forward_ms;       /* device time of the K steps of the forward pass */
+    double forward_ms;       /* device time of the forward pass (K steps and their checkpoints) */
     double total_ms;         /* wall time of the whole call */
+    double recompute_ms;     /* device time of the steps re-run from checkpoints */
+    double solve_ms;         /* device time of the adjoint Poisson solves */
     long long adj_sweeps;    /* sweeps of all adjoint Poisson solves */
     int adj_unconverged;     /* adjoint solves that stopped at adj_itmax */
     int recomputed_steps;    /* forward steps re-run from checkpoints */

@@ -81,7 +81,7 @@ class NtcfdAdjSpec(ctypes.Structure):
     _fields_ = [
         ("nsteps", ctypes.c_int), ("checkpoint_every", ctypes.c_int),
         ("w_drag", ctypes.c_double), ("w_lift", ctypes.c_double),
-        ("adj_zeta", ctypes.c_double), ("adj_itmax", ctypes.c_int),
+        ("adj_zeta", ctypes.c_double), ("adj_omega", ctypes.c_double), ("adj_itmax", ctypes.c_int),
         ("inflow_wall", ctypes.c_int), ("inflow_normal", ctypes.c_int),
         ("inflow_tangential", ctypes.c_int), ("initial_bc", ctypes.c_int),
         ("reserved", ctypes.c_int * 3),
@@ -93,6 +93,7 @@ class NtcfdAdjResult(ctypes.Structure):
         ("J", ctypes.c_double), ("dJ_dbc", (ctypes.c_double * 3) * 6),
         ("dJ_dU", ctypes.c_double), ("dJ_dtheta", ctypes.c_double),
         ("forward_ms", ctypes.c_double), ("total_ms", ctypes.c_double),
+        ("recompute_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
         ("adj_sweeps", ctypes.c_longlong), ("adj_unconverged", ctypes.c_int),
         ("recomputed_steps", ctypes.c_int), ("fwd_status", ctypes.c_int), ("pad", ctypes.c_int),
     ]

@@ -127,6 +127,17 @@ def c4(precision=FP64, **kw) -> Case:
                               steps=200, precision=precision, name="cylinder_c4", **kw)
 
 
+def uniform_inflow_state(case):
+    """Impulsive start: the inflow velocity of the Back wall in every cell
+    (u = 0, v = U sin theta, w = U cos theta), p = 0, as halo arrays."""
+    import numpy as np
+    p = case.params
+    shape = (p.nx + 4, p.ny + 4, p.nz + 4)
+    v0, w0 = p.bc_value[4][1], p.bc_value[4][2]
+    z = np.zeros(shape, order="F")
+    return (z.copy(), np.full(shape, v0, order="F"), np.full(shape, w0, order="F"), z.copy())
+
+
 C4_SEED = 20261203
 
 

@@ -625,6 +625,19 @@ __global__ void k_adj_rhs(Geom g, SorCoef<double> sc, const double* lb, double d
     if (k == 1) lw_old[c - g.pz] -= g.riDz[k] * f0;
 }
 
+// Initial guess of the next adjoint solve by linear extrapolation in time:
+// z <- 2 z - zprev, zprev <- old z (interior).
+__global__ void k_extrapolate(Geom g, double* z, double* zprev) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long c = nat(g, i, j, k);
+    const double z1 = z[c];
+    z[c] = 2.0 * z1 - zprev[c];
+    zprev[c] = z1;
+}
+
 // max |x| over the interior (the adjoint solve's tolerance is relative to it)
 template <int NT>
 __global__ void __launch_bounds__(NT) k_absmax(Geom g, const double* x, unsigned long long* slot) {

@@ -95,6 +95,8 @@ struct ntcfd_ctx {
     double time = 0.0;
     int nchunk = 0, csweeps = 1, cycle_len = 1;
     std::vector<void*> allocs;
+    void* adj_buf = nullptr;                // ntcfd_adjoint workspace, kept between calls
+    size_t adj_cap = 0;
 };
 
 namespace {
@@ -400,11 +402,11 @@ int build_graph(ntcfd_ctx* ctx) {
 // correction cycles around the resident kernel or around streaming sweeps
 // with a stop test every check_every sweeps), on pressure `p` (interior
 // updated, ghosts read) with right-hand side `b`, stop rule max|change| <=
-// zeta and sweep cap itmax.  *hc receives the final control block.
+// zeta, sweep cap itmax and relaxation omega.  *hc receives the final
+// control block.
 template <class Tc>
-int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int itmax, Ctl* hc) {
+int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int itmax, double omega, Ctl* hc) {
     const Geom g = ctx->g;
-    const ntcfd_params& P = ctx->prm;
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
@@ -425,7 +427,7 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
                                             (unsigned int*)ctx->bar);
             void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&eR,
                             (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
-                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&zeta,
+                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
                             (void*)&itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
             CK(cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
                                            dim3(kResNT), args, ctx->res_smem, st));
@@ -439,10 +441,10 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
                     k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
-                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, sub, itmax,
+                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
                         ctx->cycle_len, big_guard, ctx->slots);
                     k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
-                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, sub, itmax,
+                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
                         ctx->cycle_len, big_guard, ctx->slots);
                 }
                 k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
@@ -477,7 +479,7 @@ int run_step_eager(ntcfd_ctx* ctx) {
     k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
     k_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
     Ctl h{};
-    if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, &h)) return rc;
+    if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, P.omega, &h)) return rc;
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
     k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0, st>>>(g, pj);
@@ -790,6 +792,7 @@ void ntcfd_destroy(ntcfd_ctx* ctx) {
     if (ctx->graph) cudaGraphDestroy(ctx->graph);
     for (void* q : ctx->allocs) cudaFree(q);
     if (ctx->rec) cudaFree(ctx->rec);
+    if (ctx->adj_buf) cudaFree(ctx->adj_buf);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1345,26 +1348,25 @@ extern "C" int ntcfd_set_body_force(ntcfd_ctx* ctx, const double* fu, const doub
 // ============================================================ adjoint
 namespace {
 
-// Device storage of one ntcfd_adjoint call, released on every return path.
-struct AdjMem {
-    std::vector<void*> blocks;
-    ~AdjMem() {
-        for (void* q : blocks) cudaFree(q);
-    }
+// Workspace of ntcfd_adjoint: one device buffer kept in the context and
+// grown when a call needs more, carved into 256-byte aligned pieces.
+struct AdjCarve {
+    size_t off = 0;
+    char* base = nullptr;   // null while sizing
     template <class T>
-    cudaError_t get(T** out, size_t n) {
-        void* q = nullptr;
-        cudaError_t e = cudaMalloc(&q, n * sizeof(T) + 256);
-        if (e != cudaSuccess) return e;
-        blocks.push_back(q);
-        *out = reinterpret_cast<T*>(q);
-        return cudaSuccess;
+    void take(T** out, size_t n) {
+        off = (off + 255) & ~size_t(255);
+        *out = base ? reinterpret_cast<T*>(base + off) : nullptr;
+        off += n * sizeof(T);
     }
 };
 
 struct AdjBufs {
-    double *lu, *lv, *lw, *lp, *lpn, *lus, *lvs, *lws, *z, *badj, *lb, *wD, *wL, *lnut, *gf, *gval;
+    double *lu, *lv, *lw, *lp, *lpn, *lus, *lvs, *lws, *z, *zprev, *badj, *lb, *wD, *wL, *lnut, *gf, *gval;
     unsigned long long* slot;
+    int solves;                  // adjoint solves done (the guess extrapolates after two)
+    cudaEvent_t e0, e1;          // around each solve
+    double solve_ms;
 };
 
 // Reverse of one step: on entry lu, lv, lw, lp hold the adjoint of the state
@@ -1373,7 +1375,7 @@ struct AdjBufs {
 template <class Tc>
 int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv, const double* sw,
                  const unsigned char* guards, double scaleD, double scaleL, double zeta_rel, int itmax,
-                 long long* sweeps, int* unconverged) {
+                 double omega, long long* sweeps, int* unconverged) {
     const Geom g = ctx->g;
     const ntcfd_params& P = ctx->prm;
     cudaStream_t st = ctx->stream;
@@ -1402,14 +1404,25 @@ int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv,
     std::memcpy(&bmax, &bits, sizeof bmax);
     if (!std::isfinite(bmax)) return fail(ctx, NTCFD_ENONFINITE, "non-finite adjoint pressure right-hand side");
     if (bmax > 0.0) {
+        if (A.solves >= 2) k_extrapolate<<<g3, b3, 0, st>>>(g, A.z, A.zprev);
+        else CK(cudaMemcpyAsync(A.zprev, A.z, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
         Ctl h{};
-        if (int rc = sor_solve_eager<Tc>(ctx, A.z, A.badj, zeta_rel * bmax, itmax, &h)) return rc;
+        CK(cudaEventRecord(A.e0, st));
+        if (int rc = sor_solve_eager<Tc>(ctx, A.z, A.badj, zeta_rel * bmax, itmax, omega, &h)) return rc;
+        CK(cudaEventRecord(A.e1, st));
+        CK(cudaEventSynchronize(A.e1));
+        float sms = 0.0f;
+        CK(cudaEventElapsedTime(&sms, A.e0, A.e1));
+        A.solve_ms += sms;
+        A.solves += 1;
         if (h.timeout) return fail(ctx, NTCFD_ETIMEOUT, "the resident SOR kernel's grid barrier gave up waiting");
         if (h.nonfinite) return fail(ctx, NTCFD_ENONFINITE, "non-finite value in an adjoint SOR solve");
         *sweeps += h.ik;
         if (!h.converged) *unconverged += 1;
     } else {
         CK(cudaMemsetAsync(A.z, 0, N * sizeof(double), st));
+        CK(cudaMemsetAsync(A.zprev, 0, N * sizeof(double), st));
+        A.solves = 0;
     }
     k_adj_after_solve<<<g3, b3, 0, st>>>(g, ctx->scd, A.z, A.lb, A.lpn);
     k_adj_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, A.lb, P.dt, A.lus, A.lvs, A.lws, A.lu, A.lv, A.lw);
@@ -1441,26 +1454,55 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     const size_t G = 2 * (size_t)g.nx * g.ny + 2 * (size_t)g.nx;   // guard bytes per step
     const size_t fyz = (size_t)g.ny * g.nz, fxz = (size_t)g.nx * g.nz, fxy = (size_t)g.nx * g.ny;
     const size_t nface = 2 * (fyz + fxz + fxy);
-    AdjMem mem;
+    struct Events {
+        cudaEvent_t a = nullptr, b = nullptr, c = nullptr, d = nullptr;
+        ~Events() {
+            for (cudaEvent_t e : {a, b, c, d})
+                if (e) cudaEventDestroy(e);
+        }
+    } ev;
+    CK(cudaEventCreate(&ev.a));
+    CK(cudaEventCreate(&ev.b));
+    CK(cudaEventCreate(&ev.c));
+    CK(cudaEventCreate(&ev.d));
     double *ckpt, *blk, *fin;
     unsigned char* guards;
     AdjBufs A{};
-    CK(mem.get(&ckpt, (size_t)nck * 4 * N));
-    CK(mem.get(&blk, (size_t)M * 3 * N));
-    CK(mem.get(&fin, 4 * N + nface));
-    CK(mem.get(&guards, (size_t)K * G));
-    double** lam[] = {&A.lu, &A.lv, &A.lw, &A.lp, &A.lpn, &A.lus, &A.lvs, &A.lws, &A.z, &A.badj, &A.lb,
-                      &A.wD, &A.wL};
-    for (double** q : lam) {
-        CK(mem.get(q, N));
-        CK(cudaMemsetAsync(*q, 0, N * sizeof(double), st));
+    A.e0 = ev.a;
+    A.e1 = ev.b;
+    double** lam[] = {&A.lu, &A.lv, &A.lw, &A.lp, &A.lpn, &A.lus, &A.lvs, &A.lws, &A.z, &A.zprev, &A.badj,
+                      &A.lb, &A.wD, &A.wL};
+    auto carve = [&](AdjCarve& cv) {
+        cv.take(&ckpt, (size_t)nck * 4 * N);
+        cv.take(&blk, (size_t)M * 3 * N);
+        cv.take(&fin, 4 * N + nface);
+        cv.take(&guards, (size_t)K * G);
+        for (double** q : lam) cv.take(q, N);
+        cv.take(&A.lnut, P.LES ? N : 1);
+        cv.take(&A.gf, 3 * N);
+        cv.take(&A.gval, 18);
+        cv.take(&A.slot, 1);
+    };
+    {
+        AdjCarve sizing;
+        carve(sizing);
+        if (sizing.off > ctx->adj_cap) {
+            if (ctx->adj_buf) {
+                CK(cudaStreamSynchronize(st));
+                cudaFree(ctx->adj_buf);
+                ctx->adj_buf = nullptr;
+                ctx->adj_cap = 0;
+            }
+            CK(cudaMalloc(&ctx->adj_buf, sizing.off));
+            ctx->adj_cap = sizing.off;
+        }
+        AdjCarve real;
+        real.base = static_cast<char*>(ctx->adj_buf);
+        carve(real);
     }
-    if (P.LES) CK(mem.get(&A.lnut, N));
-    CK(mem.get(&A.gf, 3 * N));
+    for (double** q : lam) CK(cudaMemsetAsync(*q, 0, N * sizeof(double), st));
     CK(cudaMemsetAsync(A.gf, 0, 3 * N * sizeof(double), st));
-    CK(mem.get(&A.gval, 18));
     CK(cudaMemsetAsync(A.gval, 0, 18 * sizeof(double), st));
-    CK(mem.get(&A.slot, 1));
     if (int rc = prepare_steps(ctx, std::max(K, M))) return rc;
     auto save_state = [&](double* dst) -> int {
         double* src[4] = {ctx->u, ctx->v, ctx->w, ctx->p};
@@ -1493,9 +1535,16 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     // ---- forward pass: K steps, a checkpoint every M, the guards of every step
     CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), st));
     CK(cudaEventRecord(ctx->ev0, st));
+    const int last0 = (nck - 1) * M;   // first step of the last block: its states are kept here
     for (int s = 0; s < K; ++s) {
         if (s % M == 0)
             if (int rc = save_state(ckpt + (size_t)(s / M) * 4 * N)) return rc;
+        if (s >= last0) {
+            double* dst = blk + (size_t)(s - last0) * 3 * N;
+            CK(cudaMemcpyAsync(dst, ctx->u, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(dst + N, ctx->v, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(dst + 2 * N, ctx->w, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        }
         if (int rc = launch_step(ctx)) return rc;
         k_pack_guards<<<148, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, guards + (size_t)s * G);
     }
@@ -1524,15 +1573,18 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     // ---- reverse pass, block by block from the last checkpoint
     const double scaleD = sp->w_drag * (-2.0 / P.lx) / K;
     const double scaleL = sp->w_lift * (-2.0 / P.lx) / K;
-    const double zrel = sp->adj_zeta > 0 ? sp->adj_zeta : 1e-10;
+    const double zrel = sp->adj_zeta > 0 ? sp->adj_zeta : 1e-7;
     const int itmax = sp->adj_itmax > 0 ? sp->adj_itmax : 20000;
+    const double omega = sp->adj_omega > 0 ? sp->adj_omega : 1.9;
     long long sweeps = 0;
     int unconv = 0, recomputed = 0;
+    double rms = 0.0;
     for (int b = nck - 1; b >= 0; --b) {
         const int s0 = b * M, s1 = std::min(K, s0 + M);
         if (int rc = load_state(ckpt + (size_t)b * 4 * N)) return rc;
         CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), st));
-        for (int m = 0; m < s1 - s0; ++m) {
+        CK(cudaEventRecord(ev.c, st));
+        for (int m = 0; m < s1 - s0 && b < nck - 1; ++m) {
             double* dst = blk + (size_t)m * 3 * N;
             CK(cudaMemcpyAsync(dst, ctx->u, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(dst + N, ctx->v, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
@@ -1542,10 +1594,15 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
                 ++recomputed;
             }
         }
+        CK(cudaEventRecord(ev.d, st));
+        CK(cudaEventSynchronize(ev.d));
+        float bms = 0.0f;
+        CK(cudaEventElapsedTime(&bms, ev.c, ev.d));
+        rms += bms;
         for (int n = s1 - 1; n >= s0; --n) {
             const double* sb = blk + (size_t)(n - s0) * 3 * N;
             if (int rc = adjoint_step<Tc>(ctx, A, sb, sb + N, sb + 2 * N, guards + (size_t)n * G, scaleD, scaleL,
-                                          zrel, itmax, &sweeps, &unconv))
+                                          zrel, itmax, omega, &sweeps, &unconv))
                 return rc;
         }
     }
@@ -1592,6 +1649,8 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         res->dJ_dU = ga * std::cos(th) + gt * std::sin(th);
         res->dJ_dtheta = U * (-ga * std::sin(th) + gt * std::cos(th));
     }
+    res->recompute_ms = rms;
+    res->solve_ms = A.solve_ms;
     res->adj_sweeps = sweeps;
     res->adj_unconverged = unconv;
     res->recomputed_steps = recomputed;
@@ -1610,6 +1669,8 @@ extern "C" int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_a
     if (spec->nsteps < 1) return fail(ctx, NTCFD_EINVAL, "nsteps must be >= 1");
     if (spec->checkpoint_every < 1) return fail(ctx, NTCFD_EINVAL, "checkpoint_every must be >= 1");
     if (!(spec->adj_zeta >= 0.0) || spec->adj_itmax < 0) return fail(ctx, NTCFD_EINVAL, "bad adjoint stop rule");
+    if (!(spec->adj_omega >= 0.0 && spec->adj_omega < 2.0))
+        return fail(ctx, NTCFD_EINVAL, "adj_omega must be in (0, 2), or 0 for the default");
     if (!std::isfinite(spec->w_drag) || !std::isfinite(spec->w_lift))
         return fail(ctx, NTCFD_EINVAL, "non-finite objective weights");
     if (spec->initial_bc != 0 && spec->initial_bc != 1) return fail(ctx, NTCFD_EINVAL, "initial_bc must be 0 or 1");

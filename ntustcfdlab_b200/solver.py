@@ -222,7 +222,7 @@ class Solver:
         self._check(self.lib.ntcfd_set_body_force(self.h, *ptrs))
 
     def adjoint(self, nsteps: int, checkpoint_every: int, *, w_drag: float = 1.0,
-                w_lift: float = 0.0, adj_zeta: float = 0.0, adj_itmax: int = 0,
+                w_lift: float = 0.0, adj_zeta: float = 0.0, adj_itmax: int = 0, adj_omega: float = 0.0,
                 inflow=None, force_grad: bool = True, initial_bc: bool = False) -> dict:
         """Discrete adjoint of `nsteps` steps from the current state (ntcfd_adjoint).
 
@@ -236,7 +236,7 @@ class Solver:
         spec = abi.NtcfdAdjSpec()
         spec.nsteps, spec.checkpoint_every = nsteps, checkpoint_every
         spec.w_drag, spec.w_lift = w_drag, w_lift
-        spec.adj_zeta, spec.adj_itmax = adj_zeta, adj_itmax
+        spec.adj_zeta, spec.adj_itmax, spec.adj_omega = adj_zeta, adj_itmax, adj_omega
         spec.initial_bc = 1 if initial_bc else 0
         if inflow is None:
             spec.inflow_wall, spec.inflow_normal, spec.inflow_tangential = -1, 0, 1
@@ -257,6 +257,7 @@ class Solver:
             "dJ_dU": res.dJ_dU, "dJ_dtheta": res.dJ_dtheta,
             "dJ_df": grads if force_grad else None,
             "forward_ms": res.forward_ms, "total_ms": res.total_ms,
+            "recompute_ms": res.recompute_ms, "solve_ms": res.solve_ms,
             "adj_sweeps": res.adj_sweeps, "adj_unconverged": res.adj_unconverged,
             "recomputed_steps": res.recomputed_steps, "status": rc,
             "info": list(info),
