@@ -40,6 +40,12 @@ void ntcfd_gridder_unequal(int nx, int ny, int nz, double lx, double ly, double 
  * 2*npts points (z = chordwise, y = thickness) and returns that count. */
 int ntcfd_naca4_polygon(double t, int npts, double* z, double* y);
 
+/* The same with a choice of trailing edge: closed_te = 0 uses the open
+ * trailing-edge coefficient -0.1015 (as ntcfd_naca4_polygon; the points of
+ * NACA0012.DAT, read by airfoil.f90:590, follow it), closed_te = 1 the closed
+ * one, -0.1036 (the points of NACA0015.DAT follow it). */
+int ntcfd_naca4_polygon_te(double t, int npts, int closed_te, double* z, double* y);
+
 /* Closed circle of radius r centred at (0,0), npts distinct points
  * counter-clockwise from angle 0, last point = first point; returns npts+1. */
 int ntcfd_circle_polygon(double r, int npts, double* z, double* y);

@@ -185,6 +185,7 @@ SIGNATURES = {
     "ntcfd_gridder_equal": (None, [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_DP] * 9),
     "ntcfd_gridder_unequal": (None, [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [_DP] + [_DP] * 9),
     "ntcfd_naca4_polygon": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, _DP, _DP]),
+    "ntcfd_naca4_polygon_te": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, _DP, _DP]),
     "ntcfd_circle_polygon": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, _DP, _DP]),
 }
 

@@ -77,7 +77,8 @@ def c3(precision=MIXED, steps: int = 1000, **kw) -> Case:
 
 
 def c5(precision=MIXED, steps: int = 2000, **kw) -> Case:
-    """NACA0015 (analytic, t = 0.15, 256 cosine points per surface) at AoA
+    """NACA0015 (analytic, t = 0.15, closed trailing edge as in the
+    reference's NACA0015.DAT, 256 cosine points per surface) at AoA
     10 deg, 128 (span x) x 256 (y) x 384 (z) stretched grid over 1 x 8 x 16
     (12.58 M cells), body at (yc, zc) = (4, 4), Re = 5000, inflow w = 1 on the
     Back wall, Neumann outflow, periodic span, Smagorinsky Cs = 0.1, dt = 5e-4.
@@ -92,7 +93,7 @@ def c5(precision=MIXED, steps: int = 2000, **kw) -> Case:
     bcv = {"Back": (0.0, 0.0, 1.0)}
     p = make_params(nx, ny, nz, Re=5000.0, dt=f4(5e-4), LES=1, Cs=f4(0.1), precision=precision,
                     smag_mode=SMAG_REF_ALIASED, bc=bc, bc_value=bcv, lx=1.0, **kw)
-    z, y = naca4_polygon(0.15, 256)
+    z, y = naca4_polygon(0.15, 256, closed_te=True)
     return Case(name="naca0015_les", params=p, grid=grid, steps=steps,
                 mask=dict(kind="naca", az=z, ay=y, aoa=10.0, zc=4.0, yc=4.0),
                 description="NACA0015 AoA 10, 128x256x384 stretched, Re 5000, LES Cs 0.1")

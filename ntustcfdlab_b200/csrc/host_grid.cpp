@@ -103,12 +103,15 @@ extern "C" void ntcfd_gridder_unequal(int nx, int ny, int nz, double lx, double 
     metrics(nz, Z, iDz, Dzs);
 }
 
-extern "C" int ntcfd_naca4_polygon(double t, int npts, double* z, double* y) {
+extern "C" int ntcfd_naca4_polygon_te(double t, int npts, int closed_te, double* z, double* y) {
     if (npts < 2) return 0;
     const double PI = 4.0 * std::atan(1.0);
-    auto thick = [t](double x) {
+    // last coefficient of the 4-digit thickness polynomial: -0.1015 leaves the
+    // trailing edge open (NACA0012.DAT follows it), -0.1036 closes it (NACA0015.DAT)
+    const double a4 = closed_te ? -0.1036 : -0.1015;
+    auto thick = [t, a4](double x) {
         return 5.0 * t * (0.2969 * std::sqrt(x) - 0.1260 * x - 0.3516 * x * x +
-                          0.2843 * x * x * x - 0.1015 * x * x * x * x);
+                          0.2843 * x * x * x + a4 * x * x * x * x);
     };
     int q = 0;
     for (int i = 0; i < npts; ++i) {           // leading edge -> trailing edge, upper
@@ -125,6 +128,10 @@ extern "C" int ntcfd_naca4_polygon(double t, int npts, double* z, double* y) {
     }
     // the leading edge point closes the polygon: thick(0) = 0 on both sides
     return q;
+}
+
+extern "C" int ntcfd_naca4_polygon(double t, int npts, double* z, double* y) {
+    return ntcfd_naca4_polygon_te(t, npts, 0, z, y);
 }
 
 extern "C" int ntcfd_circle_polygon(double r, int npts, double* z, double* y) {

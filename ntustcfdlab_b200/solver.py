@@ -58,12 +58,13 @@ def gridder_unequal(nx, ny, nz, lx, ly, lz, band) -> dict:
     return _grid_dict(X, Y, Z, m)
 
 
-def naca4_polygon(t: float, npts: int = 256):
+def naca4_polygon(t: float, npts: int = 256, closed_te: bool = False):
     """Closed analytic NACA 4-digit symmetric section (chord 1), ordered like
-    NACA0012.DAT (LE -> upper -> TE -> lower -> LE)."""
+    NACA0012.DAT (LE -> upper -> TE -> lower -> LE).  closed_te selects the
+    closed trailing-edge coefficient (the form NACA0015.DAT follows)."""
     lib = abi.load_library()
     z, y = np.zeros(2 * npts), np.zeros(2 * npts)
-    n = lib.ntcfd_naca4_polygon(t, npts, dptr(z), dptr(y))
+    n = lib.ntcfd_naca4_polygon_te(t, npts, 1 if closed_te else 0, dptr(z), dptr(y))
     return z[:n], y[:n]
 
 
