@@ -214,6 +214,7 @@ __global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle oute
     ctl->ik = 0;
     ctl->inner = 0;
     ctl->cycles = 0;
+    ctl->restarts = 0;
     ctl->bodies = 0;
     ctl->timeout = 0;
     ctl->converged = 0;

@@ -10,7 +10,10 @@
 // publishes the updated brick-boundary rows to the global e arrays, waits at
 // a grid barrier and copies the neighbours' boundary rows of that colour
 // into its halo.  The sweep count, the stop rule (GS.f90:11,53) and the
-// final p += e run inside the kernel.
+// final p += e run inside the kernel, and so do the restarts of the
+// defect correction: when a cycle ends on its length (cycle_len sweeps), the
+// kernel adds e to p, passes a grid barrier, recomputes the FP64 defect of
+// its brick (the arithmetic of k_defect) and sweeps on from e = 0.
 //
 // The grid barrier spins with a bounded number of polls; a CTA that gives
 // up sets bar->err, and every CTA leaves the sweep loop at the next barrier,
@@ -23,8 +26,8 @@
 namespace ntcfd {
 
 struct GridBar {
-    unsigned int count;
-    unsigned int gen;
+    unsigned int count;   // arrivals (low bits) and phase (top bit), see grid_arrive
+    unsigned int gen;     // unused
     int err;
     int pad;
 };
@@ -47,6 +50,8 @@ inline size_t resident_smem(const Brick& b, int nx) {
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
+constexpr int kFill = 4;      // elements in flight per lane when a CTA walks its brick
+constexpr int kDefect = 2;    // cells in flight per lane in the in-kernel defect
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -67,29 +72,29 @@ __device__ __forceinline__ unsigned int vload(const unsigned int* p) {
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
 // Grid-wide barrier of one cooperative launch, split into arrive and wait so
-// that a CTA can work between the two.  Thread 0 of each CTA arrives with a
-// release add on the counter (after a CTA barrier, so the CTA's earlier
-// global writes are published); the last arrival resets the counter and
-// publishes the next generation with a release store.  Waiting polls the
-// generation with acquire loads, checks the shared error flag every 1024
-// polls and gives up after kBarrierPolls polls, setting the flag so that
-// every CTA leaves at its next wait.  Returns false on failure.
-__device__ __forceinline__ void grid_arrive(GridBar* b, unsigned int nblocks, unsigned int gen) {
+// that a CTA can work between the two.  One 32-bit word counts arrivals:
+// thread 0 of CTA 0 adds 2^31 - (nblocks - 1), every other CTA adds 1 (each
+// with a release add, after a CTA barrier, so the CTA's earlier global
+// writes are published).  Whatever the order, the top bit of the word flips
+// exactly when the last CTA arrives and the low bits return to their value,
+// so the word needs no reset between barriers and no second store releases
+// the waiters.  Waiting polls the word with acquire loads until its top bit
+// differs from the one this CTA's add returned, checks the shared error flag
+// every 1024 polls and gives up after kBarrierPolls polls, setting the flag
+// so that every CTA leaves at its next wait.  Returns false on failure.
+__device__ __forceinline__ void grid_arrive(GridBar* b, unsigned int nblocks, unsigned int& ticket) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        if (atom_add_release(&b->count, 1u) + 1u == nblocks) {
-            b->count = 0u;                       // ordered before the release store below
-            st_release(&b->gen, gen + 1u);
-        }
+        const unsigned int inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
+        ticket = atom_add_release(&b->count, inc);
     }
 }
 
-__device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int& gen, int* s_flag) {
+__device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int ticket, int* s_flag) {
     if (threadIdx.x == 0) {
-        const unsigned int target = gen + 1u;
         int fail = 0;
         unsigned int polls = 0;
-        while (ld_acquire(&b->gen) != target) {
+        while (((ld_acquire(&b->count) ^ ticket) & 0x80000000u) == 0u) {
             if ((++polls & 1023u) == 0u) {
                 if (vload(&b->err) != 0) { fail = 1; break; }
                 if (polls > kBarrierPolls) {
@@ -102,27 +107,46 @@ __device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int& gen, int* s_
         *s_flag = fail;
     }
     __syncthreads();
-    gen += 1u;
     return *s_flag == 0;
 }
 
-__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int nblocks, unsigned int& gen,
-                                          int* s_flag) {
-    grid_arrive(b, nblocks, gen);
-    return grid_wait(b, gen, s_flag);
+__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int nblocks, int* s_flag) {
+    unsigned int ticket = 0;
+    grid_arrive(b, nblocks, ticket);
+    return grid_wait(b, ticket, s_flag);
 }
 
-template <class Tc, int NT>
+// Row e of a brick's edge ring (jl or kl on the brick boundary), for e < ne,
+// or of its interior, for e >= ne; nj x nk rows, ni = interior rows.
+__device__ __forceinline__ void brick_row(int e, int nj, int nk, int ni, int ne, int& jl, int& kl) {
+    if (ni == 0) {                       // every row is an edge row
+        jl = e % nj + 1;
+        kl = e / nj + 1;
+    } else if (e >= ne) {                // interior: (nj-2) x (nk-2) rows
+        const int q = e - ne;
+        jl = q % (nj - 2) + 2;
+        kl = q / (nj - 2) + 2;
+    } else if (e < 2 * nj) {             // first and last k-row of the brick
+        jl = e % nj + 1;
+        kl = e < nj ? 1 : nk;
+    } else {                             // first and last j-row, inner k
+        const int q = e - 2 * nj;
+        kl = q % (nk - 2) + 2;
+        jl = q < nk - 2 ? 1 : nj;
+    }
+}
+
+template <class Tc, int NT, bool CD, bool CR>
 __global__ void __launch_bounds__(NT, 1)
-k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __restrict__ eRg,
-               Tc* __restrict__ eBg, const Tc* __restrict__ dRg, const Tc* __restrict__ dBg,
+k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const double* __restrict__ b,
+               Tc* __restrict__ eRg,
+               Tc* __restrict__ eBg, Tc* __restrict__ dRg, Tc* __restrict__ dBg,
                const Tc* __restrict__ rdRg, const Tc* __restrict__ rdBg, Ctl* ctl, GridBar* bar,
                double omega, double zeta, int itmax, int cycle_len, int check_every,
                unsigned long long* ring) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using B = decltype(abs_bits(Tc(0)));
     __shared__ int s_flag;
-    __shared__ unsigned int s_gen;
     __shared__ unsigned long long s_ring;
     __shared__ B s_red[NT / 32];
     const int JB = br.JB, KB = br.KB, mx = br.mx;
@@ -142,7 +166,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
     Tc* const cBs = cFs + KB;
     Tc* const D0 = cBs + KB;
     Tc* const D1 = D0 + brick;
-    Tc* const R0 = br.cache_d ? D1 + brick : D0;
+    Tc* const R0 = CD ? D1 + brick : D0;
     Tc* const R1 = R0 + brick;
     constexpr int NWARP = NT / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -170,30 +194,75 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
         cFs[q] = sc.cF[k];
         cBs[q] = sc.cB[k];
     }
-    if (br.cache_d || br.cache_rd) {
-        for (int q = tid; q < nj * nk * mx; q += NT) {
-            const int m = q % mx;
-            const int row = q / mx;
+    if (CD || CR) {
+        // one warp per row, lanes along m, kFill elements of each array in flight per lane
+        for (int row = warp; row < nj * nk; row += NT / 32) {
             const int jl = row % nj, kl = row / nj;
-            const long long gq = spl(g, m, j0 + jl, k0 + kl);
-            const int sq = (kl * JB + jl) * mx + m;
-            if (br.cache_d) { D0[sq] = dRg[gq]; D1[sq] = dBg[gq]; }
-            if (br.cache_rd) { R0[sq] = rdRg[gq]; R1[sq] = rdBg[gq]; }
+            const long long gq0 = spl(g, 0, j0 + jl, k0 + kl);
+            const int sq0 = (kl * JB + jl) * mx;
+            for (int m0 = 0; m0 < mx; m0 += 32 * kFill) {
+                Tc a0[kFill], a1[kFill], a2[kFill], a3[kFill];
+#pragma unroll
+                for (int u = 0; u < kFill; ++u) {
+                    const int m = m0 + lane + 32 * u;
+                    if (m < mx) {
+                        if (CD) { a0[u] = dRg[gq0 + m]; a1[u] = dBg[gq0 + m]; }
+                        if (CR) { a2[u] = rdRg[gq0 + m]; a3[u] = rdBg[gq0 + m]; }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kFill; ++u) {
+                    const int m = m0 + lane + 32 * u;
+                    if (m < mx) {
+                        if (CD) { D0[sq0 + m] = a0[u]; D1[sq0 + m] = a1[u]; }
+                        if (CR) { R0[sq0 + m] = a2[u]; R1[sq0 + m] = a3[u]; }
+                    }
+                }
+            }
         }
     }
-    if (tid == 0) s_gen = vload(&bar->gen);
     __syncthreads();
-    unsigned int gen = s_gen;
+    unsigned int ticket = 0;   // thread 0: the barrier word before this CTA's last arrival
     const unsigned int nblocks = gridDim.x;
     const int ik0 = ctl->ik;
     const int nrows = nj * nk;
+    const int ni = (nj > 2 && nk > 2) ? (nj - 2) * (nk - 2) : 0;   // interior rows
+    const int ne = nrows - ni;                                       // edge rows
     const Tc om = (Tc)omega;
-    int done = 0;
+    int done = 0;        // sweeps of this launch
+    int done_c = 0;      // sweeps of the current cycle
+    int restarts = 0;
     bool conv = false, nonfinite = false, failed = false;
     double last = 0.0;
+    // p += e over the brick (natural <- shared memory)
+    // (one warp per row, lanes along i, kFill values of p in flight per lane)
+    auto add_e_to_p = [&]() {
+        for (int row = warp; row < nrows; row += NWARP) {
+            const int jl = row % nj + 1, kl = row / nj + 1;
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const long long c0 = nat(g, 0, j, k);
+            const int sr = (kl * RS + jl) * mx;
+            for (int i0 = 1; i0 <= g.nx; i0 += 32 * kFill) {
+                double pv[kFill];
+#pragma unroll
+                for (int u = 0; u < kFill; ++u) {
+                    const int i = i0 + lane + 32 * u;
+                    if (i <= g.nx) pv[u] = p[c0 + i];
+                }
+#pragma unroll
+                for (int u = 0; u < kFill; ++u) {
+                    const int i = i0 + lane + 32 * u;
+                    if (i <= g.nx) p[c0 + i] = pv[u] + (double)(((i + j + k) & 1) ? S1 : S0)[sr + ((i + 2) >> 1)];
+                }
+            }
+        }
+    };
 
-    for (int s = 0; ik0 + s < itmax && s < cycle_len; ++s) {
-        if (blockIdx.x == 0 && tid == 0) ring[(s + 1) % 3] = 0ULL;
+  for (;;) {
+    done_c = 0;
+    for (int s = 0; ik0 + done + s < itmax && s < cycle_len; ++s) {
+        const int sg = done + s;   // sweep of this launch: ring slot
+        if (blockIdx.x == 0 && tid == 0) ring[(sg + 1) % 3] = 0ULL;
         B ch = B(0);
         for (int c = 0; c < 2 && !failed; ++c) {
             Tc* W = c ? S1 : S0;
@@ -207,10 +276,12 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
             // first the brick-edge rows, which the neighbours need, then arrive
             // at the grid barrier, then the interior rows, then wait.
             for (int pass = 0; pass < 2; ++pass) {
-                int jl = nj > 0 ? warp % nj + 1 : 1, kl = nj > 0 ? warp / nj + 1 : 1;
-                for (int row = warp; row < nrows; row += NWARP) {
-                    const bool edge = (jl == 1 || jl == nj || kl == 1 || kl == nk);
-                    if (edge == (pass == 0)) {
+                const bool edge = pass == 0;
+                const int e0r = edge ? 0 : ne, e1r = edge ? ne : nrows;
+                for (int er = e0r + warp; er < e1r; er += NWARP) {
+                    int jl, kl;
+                    brick_row(er, nj, nk, ni, ne, jl, kl);
+                    {
                         const int j = j0 + jl - 1, k = k0 + kl - 1;
                         const int r = ((j + k) ^ c) & 1;
                         const int sr = (kl * RS + jl) * mx;
@@ -224,8 +295,10 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
                             const int so = sr + m;
                             const Tc sum = cEs[i] * O[so + r] + cWs[i] * O[so - 1 + r] + cN * O[so + mx] +
                                            cS * O[so - mx] + cF * O[so + plane] + cB * O[so - plane];
-                            const Tc rd = br.cache_rd ? Rs[dr + m] : __ldg(Rg + gr + m);
-                            const Tc dv = br.cache_d ? Ds[dr + m] : __ldg(Dg + gr + m);
+                            const Tc rd = CR ? Rs[dr + m] : __ldg(Rg + gr + m);
+                            // d may be rewritten by a restart of this launch, by this CTA only:
+                            // a plain (L1-coherent) load, not the read-only path
+                            const Tc dv = CD ? Ds[dr + m] : __ldca(Dg + gr + m);
                             const Tc e0 = W[so];
                             const Tc diff = (rd * sum + dv) - e0;
                             const Tc e1 = e0 + om * diff;
@@ -235,11 +308,9 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
                             ch = db > ch ? db : ch;
                         }
                     }
-                    jl += NWARP;
-                    while (jl > nj) { jl -= nj; ++kl; }
                 }
                 // red half: arrive once the edge rows are out, wait after the interior
-                if (pass == 0 && c == 0) grid_arrive(bar, nblocks, gen);
+                if (pass == 0 && c == 0) grid_arrive(bar, nblocks, ticket);
             }
             if (c == 1) {
                 // this CTA's max |change| over the sweep -> ring slot of sweep s
@@ -257,16 +328,16 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
                         const B t2 = __shfl_xor_sync(0xffffffffu, b2, o);
                         b2 = t2 > b2 ? t2 : b2;
                     }
-                    if (tid == 0 && b2 != B(0)) atomicMax(&ring[s % 3], widen_bits(b2));
+                    if (tid == 0 && b2 != B(0)) atomicMax(&ring[sg % 3], widen_bits(b2));
                 }
                 // black half: a full barrier, so that every CTA's max (interior
                 // rows included) is in the ring before anyone reads it
-                if (!grid_sync(bar, nblocks, gen, &s_flag)) {
+                if (!grid_sync(bar, nblocks, &s_flag)) {
                     failed = true;
                     break;
                 }
-                if (tid == 0) s_ring = *(volatile unsigned long long*)&ring[s % 3];
-            } else if (!grid_wait(bar, gen, &s_flag)) {
+                if (tid == 0) s_ring = *(volatile unsigned long long*)&ring[sg % 3];
+            } else if (!grid_wait(bar, ticket, &s_flag)) {
                 failed = true;
                 break;
             }
@@ -285,8 +356,8 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
             __syncthreads();
         }
         if (failed) break;
-        done = s + 1;
-        const int ik = ik0 + done;
+        done_c = s + 1;
+        const int ik = ik0 + done + done_c;
         if (ik % check_every == 0 || ik >= itmax) {
             const unsigned long long bits = s_ring;
             last = __longlong_as_double((long long)bits);
@@ -295,18 +366,68 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, Tc* __r
             if (conv || nonfinite) break;
         }
     }
-    // p += e over the brick (natural <- shared memory)
-    for (int it = tid; it < nj * nk * g.nx; it += NT) {
-        const int i = it % g.nx + 1;
-        const int row = it / g.nx;
-        const int jl = row % nj + 1, kl = row / nj + 1;
-        const int j = j0 + jl - 1, k = k0 + kl - 1;
-        const int col = (i + j + k) & 1;
-        p[nat(g, i, j, k)] += (double)(col ? S1 : S0)[(kl * RS + jl) * mx + ((i + 2) >> 1)];
+    done += done_c;
+    // another cycle only when this one ended on its length
+    if (failed || conv || nonfinite || done_c < cycle_len || ik0 + done >= itmax) break;
+    // restart: p += e, then the FP64 defect from the updated p, with e = 0
+    add_e_to_p();
+    __syncthreads();
+    for (int q = tid; q < 2 * tile; q += NT) S0[q] = Tc(0);
+    if (!grid_sync(bar, nblocks, &s_flag)) {
+        failed = true;
+        break;
     }
+    {
+        // one warp per row, lanes along i, kDefect cells in flight per lane; p of this
+        // launch's other CTAs is read from L2
+        const SorCoef<double> scd{g.cE, g.cW, g.cN, g.cS, g.cF, g.cB};
+        for (int row = warp; row < nrows; row += NWARP) {
+            const int jl = row % nj + 1, kl = row / nj + 1;
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const long long c0 = nat(g, 0, j, k);
+            const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
+            const long long g0 = spl(g, 0, j, k);
+            for (int i0 = 1; i0 <= g.nx; i0 += 32 * kDefect) {
+                double pe[kDefect], pw[kDefect], pn[kDefect], ps[kDefect], pf[kDefect], pb[kDefect],
+                    pc[kDefect], bc[kDefect];
+#pragma unroll
+                for (int u = 0; u < kDefect; ++u) {
+                    const int i = min(i0 + lane + 32 * u, g.nx);
+                    const long long c = c0 + i;
+                    pe[u] = __ldcg(p + c + 1);
+                    pw[u] = __ldcg(p + c - 1);
+                    pn[u] = __ldcg(p + c + g.px);
+                    ps[u] = __ldcg(p + c - g.px);
+                    pf[u] = __ldcg(p + c + g.pz);
+                    pb[u] = __ldcg(p + c - g.pz);
+                    pc[u] = __ldcg(p + c);
+                    bc[u] = __ldg(b + c);
+                }
+#pragma unroll
+                for (int u = 0; u < kDefect; ++u) {
+                    const int i = i0 + lane + 32 * u;
+                    if (i > g.nx) continue;
+                    const double sv = scd.cE[i] * pe[u] + scd.cW[i] * pw[u] + scd.cN[j] * pn[u] +
+                                      scd.cS[j] * ps[u] + scd.cF[k] * pf[u] + scd.cB[k] * pb[u];
+                    const double dval = rdiag_of(scd, i, j, k) * sv - bc[u] - pc[u];
+                    const int m = (i + 2) >> 1;
+                    const bool red = ((i + j + k) & 1) == 0;
+                    if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
+                    else (red ? dRg : dBg)[g0 + m] = (Tc)dval;
+                }
+            }
+        }
+    }
+    // the next half-sweep reads d only of this CTA's own cells
+    __syncthreads();
+    ++restarts;
+  }
+    add_e_to_p();
     if (blockIdx.x == 0 && tid == 0) {
         ctl->ik = ik0 + done;
-        ctl->inner = done;
+        ctl->inner = done_c;
+        ctl->cycles += restarts;
+        ctl->restarts += restarts;
         ctl->bodies += done;
         if (done > 0) ctl->last_change = last;
         if (conv) ctl->converged = 1;

@@ -214,6 +214,18 @@ SorCoef<double> sor_coef<double>(ntcfd_ctx* ctx) { return ctx->scd; }
 template <>
 SorCoef<float> sor_coef<float>(ntcfd_ctx* ctx) { return ctx->scf; }
 
+// The resident SOR kernel for a brick plan (d and rd cached or not).
+template <class Tc>
+using ResidentFn = void (*)(Geom, SorCoef<Tc>, Brick, double*, const double*, Tc*, Tc*, Tc*, Tc*, const Tc*,
+                            const Tc*, Ctl*, GridBar*, double, double, int, int, int, unsigned long long*);
+template <class Tc>
+ResidentFn<Tc> resident_kernel(const Brick& b) {
+    if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true>;
+    if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false>;
+    if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true>;
+    return k_sor_resident<Tc, kResNT, false, false>;
+}
+
 // Brick plan of the resident SOR kernel: the split of the (j,k) rows into at
 // most (SM count) bricks that minimises the largest brick, under the shared
 // memory limit (e of both colours for the brick and a one-row halo, plus d
@@ -251,7 +263,7 @@ bool plan_resident(ntcfd_ctx* ctx) {
         }
     }
     if (best < 0) return false;
-    auto kern = k_sor_resident<Tc, kResNT>;
+    auto kern = resident_kernel<Tc>(bb);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm) != cudaSuccess) {
         cudaGetLastError();
         return false;
@@ -317,9 +329,9 @@ int build_graph(ntcfd_ctx* ctx) {
                       (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, (cudaGraphConditionalHandle)0, 0,
                       ctx->ring, (unsigned int*)ctx->bar));
         od = {m};
-        GK(add_kernel_ex(&m, outer, od, k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid), dim3(kResNT),
-                         ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, eR, eB,
-                         (const Tc*)dR, (const Tc*)dB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
+        GK(add_kernel_ex(&m, outer, od, resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid), dim3(kResNT),
+                         ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, (const double*)ctx->b,
+                         eR, eB, dR, dB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
                          ctx->bar, P.omega, P.zeta, P.itmax, ctx->cycle_len, ctx->csweeps, ctx->ring));
         od = {m};
         GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
@@ -425,11 +437,11 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         if (ctx->resident) {
             k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, ctx->ring,
                                             (unsigned int*)ctx->bar);
-            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&eR,
+            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&b, (void*)&eR,
                             (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
                             (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
                             (void*)&itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
-            CK(cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
+            CK(cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
                                            dim3(kResNT), args, ctx->res_smem, st));
         } else {
             k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, nullptr,
@@ -634,12 +646,13 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
                  int zero = 0;
                  (void)zero;
                  cudaMemsetAsync(&ctx->ctl->ik, 0, sizeof(int), ctx->stream);
-                 void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&eR,
+                 void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&ctx->b,
+                                 (void*)&eR,
                                  (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
                                  (void*)&ctx->ctl, (void*)&ctx->bar,
                                  (void*)&P.omega, (void*)&kZeroZeta, (void*)&nsw, (void*)&nsw,
                                  (void*)&kOne, (void*)&ctx->ring};
-                 cudaLaunchCooperativeKernel((const void*)k_sor_resident<Tc, kResNT>, dim3(ctx->res_grid),
+                 cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
                                              dim3(kResNT), args, ctx->res_smem, ctx->stream);
              }, &out->resident_ms, 1)))
             return rc;

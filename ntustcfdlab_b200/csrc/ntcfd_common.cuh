@@ -61,7 +61,8 @@ struct Ctl {
     int bodies;                   // inner loop bodies run in this step
     int timeout;                  // a bounded device wait gave up
     int pad_stop, pad_more;       // the last loop decisions (read by the host in eager mode)
-    int pad2[2];
+    int restarts;                 // correction cycles restarted inside the resident SOR kernel
+    int pad2;
     double last_change;           // value of the last tested sweep
     double cdrag, clift, divmax;
 };
