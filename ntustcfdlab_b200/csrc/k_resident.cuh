@@ -45,8 +45,11 @@ template <class Tc>
 inline size_t resident_smem(const Brick& b, int nx) {
     const size_t tile = (size_t)(b.JB + 2) * (b.KB + 2) * b.mx;
     const size_t brick = (size_t)b.JB * b.KB * b.mx;
-    return sizeof(Tc) * (2 * tile + 2 * (size_t)(nx + 4) + 2 * (size_t)(b.JB + b.KB) +
-                         (b.cache_d ? 2 * brick : 0) + (b.cache_rd ? 2 * brick : 0));
+    const size_t arrays = sizeof(Tc) * (2 * tile + 2 * (size_t)(nx + 4) + 2 * (size_t)(b.JB + b.KB) +
+                                        (b.cache_d ? 2 * brick : 0) + (b.cache_rd ? 2 * brick : 0));
+    // + row table (int4 offsets and four coefficients per row) and halo table (int2 per row)
+    const size_t rows = (size_t)b.JB * b.KB;
+    return ((arrays + 15) & ~size_t(15)) + rows * (16 + 4 * sizeof(Tc)) + 8 * (size_t)(2 * (b.JB + b.KB));
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
@@ -168,6 +171,15 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     Tc* const D1 = D0 + brick;
     Tc* const R0 = CD ? D1 + brick : D0;
     Tc* const R1 = R0 + brick;
+    Tc* const arrays_end = CR ? R1 + brick : (CD ? D1 + brick : D0);
+    // row table: per row of the brick, in sweep order (edge rows first), the shared-memory
+    // tile row, the brick row of d/rd, the global colour-split row and (j+k)&1, and the
+    // row's cN, cS, cF, cB; halo table: per halo row, global source row (-1: domain ghost)
+    // and tile row
+    const size_t toff = ((size_t)((unsigned char*)arrays_end - smem_raw) + 15) & ~size_t(15);
+    int4* const rowT = reinterpret_cast<int4*>(smem_raw + toff);
+    Tc* const rowC = reinterpret_cast<Tc*>(rowT + JB * KB);
+    int2* const haloT = reinterpret_cast<int2*>(rowC + 4 * JB * KB);
     constexpr int NWARP = NT / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tid = threadIdx.x;
@@ -193,6 +205,29 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         const int k = min(k0 + q, g.nz);
         cFs[q] = sc.cF[k];
         cBs[q] = sc.cB[k];
+    }
+    {
+        const int nr = nj * nk;
+        const int nin = (nj > 2 && nk > 2) ? (nj - 2) * (nk - 2) : 0;
+        for (int er = tid; er < nr; er += NT) {
+            int jl, kl;
+            brick_row(er, nj, nk, nin, nr - nin, jl, kl);
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            rowT[er] = make_int4((kl * RS + jl) * mx, ((kl - 1) * JB + (jl - 1)) * mx,
+                                 ys * (j + 1) + zs * (k + 1), (j + k) & 1);
+            rowC[4 * er + 0] = sc.cN[j];
+            rowC[4 * er + 1] = sc.cS[j];
+            rowC[4 * er + 2] = sc.cF[k];
+            rowC[4 * er + 3] = sc.cB[k];
+        }
+        for (int h = tid; h < 2 * nk + 2 * nj; h += NT) {
+            int jl, kl;
+            if (h < 2 * nk) { kl = h % nk + 1; jl = (h < nk) ? 0 : nj + 1; }
+            else { const int h2 = h - 2 * nk; jl = h2 % nj + 1; kl = (h2 < nj) ? 0 : nk + 1; }
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const bool in = j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;   // domain ghosts stay 0
+            haloT[h] = make_int2(in ? ys * (j + 1) + zs * (k + 1) : -1, (kl * RS + jl) * mx);
+        }
     }
     if (CD || CR) {
         // one warp per row, lanes along m, kFill elements of each array in flight per lane
@@ -279,33 +314,46 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 const bool edge = pass == 0;
                 const int e0r = edge ? 0 : ne, e1r = edge ? ne : nrows;
                 for (int er = e0r + warp; er < e1r; er += NWARP) {
-                    int jl, kl;
-                    brick_row(er, nj, nk, ni, ne, jl, kl);
-                    {
-                        const int j = j0 + jl - 1, k = k0 + kl - 1;
-                        const int r = ((j + k) ^ c) & 1;
-                        const int sr = (kl * RS + jl) * mx;
-                        const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
-                        const int gr = ys * (j + 1) + zs * (k + 1);
-                        const Tc cN = cNs[jl - 1], cS = cSs[jl - 1], cF = cFs[kl - 1], cB = cBs[kl - 1];
-                        for (int t = lane; t < half; t += 32) {
-                            const int i = 2 * t + 2 - r;
-                            if (i > g.nx) break;
-                            const int m = t + 2 - r;
-                            const int so = sr + m;
-                            const Tc sum = cEs[i] * O[so + r] + cWs[i] * O[so - 1 + r] + cN * O[so + mx] +
-                                           cS * O[so - mx] + cF * O[so + plane] + cB * O[so - plane];
-                            const Tc rd = CR ? Rs[dr + m] : __ldg(Rg + gr + m);
-                            // d may be rewritten by a restart of this launch, by this CTA only:
-                            // a plain (L1-coherent) load, not the read-only path
-                            const Tc dv = CD ? Ds[dr + m] : __ldca(Dg + gr + m);
-                            const Tc e0 = W[so];
-                            const Tc diff = (rd * sum + dv) - e0;
-                            const Tc e1 = e0 + om * diff;
-                            W[so] = e1;
-                            if (edge) Ec[gr + m] = e1;
-                            const B db = abs_bits(diff);
-                            ch = db > ch ? db : ch;
+                    const int4 rt = rowT[er];
+                    const int sr = rt.x, dr = rt.y, gr = rt.z, r = rt.w ^ c;
+                    const Tc cN = rowC[4 * er], cS = rowC[4 * er + 1], cF = rowC[4 * er + 2],
+                             cB = rowC[4 * er + 3];
+                    // two cells per lane (t and t + 32), every load issued before any store
+                    for (int t0 = lane; t0 < half; t0 += 64) {
+                        const int tB = t0 + 32;
+                        const int iA = 2 * t0 + 2 - r, iB0 = 2 * tB + 2 - r;
+                        if (iA > g.nx) break;
+                        const bool okB = tB < half && iB0 <= g.nx;
+                        const int mA = t0 + 2 - r, mB = okB ? tB + 2 - r : mA;
+                        const int iB = okB ? iB0 : iA;
+                        const int sA = sr + mA, sB = sr + mB;
+                        const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
+                        const Tc oEA = O[sA + r], oWA = O[sA - 1 + r], oNA = O[sA + mx], oSA = O[sA - mx],
+                                 oFA = O[sA + plane], oBA = O[sA - plane];
+                        const Tc oEB = O[sB + r], oWB = O[sB - 1 + r], oNB = O[sB + mx], oSB = O[sB - mx],
+                                 oFB = O[sB + plane], oBB = O[sB - plane];
+                        const Tc rdA = CR ? Rs[dr + mA] : __ldg(Rg + gr + mA);
+                        const Tc rdB = CR ? Rs[dr + mB] : __ldg(Rg + gr + mB);
+                        // d may be rewritten by a restart of this launch, by this CTA only:
+                        // a plain (L1-coherent) load, not the read-only path
+                        const Tc dvA = CD ? Ds[dr + mA] : __ldca(Dg + gr + mA);
+                        const Tc dvB = CD ? Ds[dr + mB] : __ldca(Dg + gr + mB);
+                        const Tc e0A = W[sA], e0B = W[sB];
+                        const Tc sumA = eA * oEA + wA * oWA + cN * oNA + cS * oSA + cF * oFA + cB * oBA;
+                        const Tc sumB = eB * oEB + wB * oWB + cN * oNB + cS * oSB + cF * oFB + cB * oBB;
+                        const Tc diffA = (rdA * sumA + dvA) - e0A;
+                        const Tc diffB = (rdB * sumB + dvB) - e0B;
+                        const Tc e1A = e0A + om * diffA;
+                        const Tc e1B = e0B + om * diffB;
+                        W[sA] = e1A;
+                        if (edge) Ec[gr + mA] = e1A;
+                        const B dbA = abs_bits(diffA);
+                        ch = dbA > ch ? dbA : ch;
+                        if (okB) {
+                            W[sB] = e1B;
+                            if (edge) Ec[gr + mB] = e1B;
+                            const B dbB = abs_bits(diffB);
+                            ch = dbB > ch ? dbB : ch;
                         }
                     }
                 }
@@ -341,17 +389,26 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 failed = true;
                 break;
             }
-            // neighbours' boundary rows of colour c into the halo, one warp per row
+            // neighbours' boundary rows of colour c into the halo, one warp per row;
+            // L2 reads (ld.global.cg): the rows were written by other CTAs this half-sweep
             for (int h = warp; h < 2 * nk + 2 * nj; h += NWARP) {
-                int jl, kl;
-                if (h < 2 * nk) { kl = h % nk + 1; jl = (h < nk) ? 0 : nj + 1; }
-                else { const int h2 = h - 2 * nk; jl = h2 % nj + 1; kl = (h2 < nj) ? 0 : nk + 1; }
-                const int j = j0 + jl - 1, k = k0 + kl - 1;
-                if (j < 1 || j > g.ny || k < 1 || k > g.nz) continue;   // domain ghosts stay 0
-                const Tc* src = Ec + spl(g, 0, j, k);
-                Tc* dst = W + (kl * RS + jl) * mx;
-                // L2 reads (ld.global.cg): the rows were written by other CTAs this half-sweep
-                for (int m = lane; m < mx; m += 32) dst[m] = __ldcg(src + m);
+                const int2 ht = haloT[h];
+                if (ht.x < 0) continue;
+                const Tc* src = Ec + ht.x;
+                Tc* dst = W + ht.y;
+                for (int m0 = 0; m0 < mx; m0 += 32 * kFill) {
+                    Tc v[kFill];
+#pragma unroll
+                    for (int u = 0; u < kFill; ++u) {
+                        const int m = m0 + lane + 32 * u;
+                        if (m < mx) v[u] = __ldcg(src + m);
+                    }
+#pragma unroll
+                    for (int u = 0; u < kFill; ++u) {
+                        const int m = m0 + lane + 32 * u;
+                        if (m < mx) dst[m] = v[u];
+                    }
+                }
             }
             __syncthreads();
         }
