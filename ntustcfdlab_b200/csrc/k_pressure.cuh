@@ -56,18 +56,29 @@ __global__ void __launch_bounds__(256) k_rhs(Geom g, SorCoef<double> sc, const d
 // Tc; e reset to 0.  Inside the step graph (in_graph = 1) it also arms the
 // inner loop's condition.
 // For the resident path (ring != null) it also clears the ring of sweep
-// maxima and the grid barrier the next kernel uses.
+// maxima and the grid barrier the next kernel uses, and with begin = 1 it
+// starts the solve (the counters k_sor_begin resets).
 template <class Tc>
 __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, const double* p,
                                                 const double* b, Tc* dR, Tc* dB, Tc* eR, Tc* eB,
                                                 Ctl* ctl, cudaGraphConditionalHandle inner,
                                                 int in_graph, unsigned long long* ring,
-                                                unsigned int* bar) {
+                                                unsigned int* bar, int begin) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (blockIdx.x == 0 && blockIdx.y == 0 && blockIdx.z == 0 && threadIdx.x == 0 &&
         threadIdx.y == 0 && threadIdx.z == 0) {
+        if (begin) {
+            ctl->ik = 0;
+            ctl->cycles = 0;
+            ctl->restarts = 0;
+            ctl->bodies = 0;
+            ctl->timeout = 0;
+            ctl->converged = 0;
+            ctl->nonfinite = 0;
+            ctl->last_change = 0.0;
+        }
         ctl->inner = 0;
         if (in_graph) cudaGraphSetConditional(inner, 1u);
         if (ring) { ring[0] = 0ULL; ring[1] = 0ULL; ring[2] = 0ULL; }

@@ -426,13 +426,13 @@ __global__ void __launch_bounds__(NT) k_divmax(Geom g, const double* u, const do
     block_max_atomic<NT>(d, slot);  // one slot: the diagnostic runs once per step
 }
 
-// Records the step; `fixed` kernels per step, 3 per correction cycle (cycles
-// restarted inside the resident SOR kernel launch nothing) and 2*csweeps + 1
-// per inner loop body.
+// Records the step; `fixed` kernels per step, per_cycle per correction cycle
+// (cycles restarted inside the resident SOR kernel launch nothing) and
+// per_body per inner loop body.
 __global__ void k_step_end(Ctl* ctl, StepRec* rec, unsigned long long* divslot, int diag,
-                           int fixed, int per_body) {
+                           int fixed, int per_cycle, int per_body) {
     const int s = ctl->step;
-    rec[s].launches = fixed + 3 * (ctl->cycles - ctl->restarts) + ctl->bodies * per_body;
+    rec[s].launches = fixed + per_cycle * (ctl->cycles - ctl->restarts) + ctl->bodies * per_body;
     rec[s].timeout = ctl->timeout;
     rec[s].sor_iters = ctl->ik;
     rec[s].converged = ctl->converged;

@@ -9,8 +9,9 @@
 // A half-sweep updates the CTA's cells of one colour from shared memory,
 // publishes the updated brick-boundary rows to the global e arrays, waits at
 // a grid barrier and copies the neighbours' boundary rows of that colour
-// into its halo.  The sweep count, the stop rule (GS.f90:11,53) and the
-// final p += e run inside the kernel, and so do the restarts of the
+// into its halo.  The sweep count, the stop rule (GS.f90:11,53), the count
+// of correction cycles and the final p += e run inside the kernel, and so do
+// the restarts of the
 // defect correction: when a cycle ends on its length (cycle_len sweeps), the
 // kernel adds e to p, passes a grid barrier, recomputes the FP64 defect of
 // its brick (the arithmetic of k_defect) and sweeps on from e = 0.
@@ -55,6 +56,7 @@ inline size_t resident_smem(const Brick& b, int nx) {
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
 constexpr int kFill = 4;      // elements in flight per lane when a CTA walks its brick
 constexpr int kDefect = 2;    // cells in flight per lane in the in-kernel defect
+constexpr int kHalo = 8;      // halo elements in flight per thread
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -389,25 +391,30 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 failed = true;
                 break;
             }
-            // neighbours' boundary rows of colour c into the halo, one warp per row;
-            // L2 reads (ld.global.cg): the rows were written by other CTAs this half-sweep
-            for (int h = warp; h < 2 * nk + 2 * nj; h += NWARP) {
-                const int2 ht = haloT[h];
-                if (ht.x < 0) continue;
-                const Tc* src = Ec + ht.x;
-                Tc* dst = W + ht.y;
-                for (int m0 = 0; m0 < mx; m0 += 32 * kFill) {
-                    Tc v[kFill];
+            // neighbours' boundary rows of colour c into the halo, flattened over the CTA
+            // so that each thread has all its L2 reads (ld.global.cg: the rows were
+            // written by other CTAs this half-sweep) in flight at once
+            {
+                const int tot = (2 * nk + 2 * nj) * mx;
+                for (int q0 = 0; q0 < tot; q0 += NT * kHalo) {
+                    Tc v[kHalo];
+                    int dst[kHalo];
 #pragma unroll
-                    for (int u = 0; u < kFill; ++u) {
-                        const int m = m0 + lane + 32 * u;
-                        if (m < mx) v[u] = __ldcg(src + m);
+                    for (int u = 0; u < kHalo; ++u) {
+                        const int q = q0 + u * NT + tid;
+                        dst[u] = -1;
+                        if (q < tot) {
+                            const int h = q / mx, m = q - h * mx;
+                            const int2 ht = haloT[h];
+                            if (ht.x >= 0) {
+                                v[u] = __ldcg(Ec + ht.x + m);
+                                dst[u] = ht.y + m;
+                            }
+                        }
                     }
 #pragma unroll
-                    for (int u = 0; u < kFill; ++u) {
-                        const int m = m0 + lane + 32 * u;
-                        if (m < mx) dst[m] = v[u];
-                    }
+                    for (int u = 0; u < kHalo; ++u)
+                        if (dst[u] >= 0) W[dst[u]] = v[u];
                 }
             }
             __syncthreads();
@@ -483,7 +490,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     if (blockIdx.x == 0 && tid == 0) {
         ctl->ik = ik0 + done;
         ctl->inner = done_c;
-        ctl->cycles += restarts;
+        ctl->cycles += restarts + (itmax > 0 ? 1 : 0);   // the launch's cycles, the last included
         ctl->restarts += restarts;
         ctl->bodies += done;
         if (done > 0) ctl->last_change = last;

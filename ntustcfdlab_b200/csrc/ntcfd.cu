@@ -308,13 +308,6 @@ int build_graph(ntcfd_ctx* ctx) {
                   (const double*)ctx->v, (const double*)ctx->w, (const double*)ctx->us,
                   (const double*)ctx->vs, (const double*)ctx->ws, ctx->b, P.dt));
     dep = {n};
-    cudaGraphConditionalHandle hout, hin;
-    GK(cudaGraphConditionalHandleCreate(&hout, G, 0, 0));
-    GK(add_kernel(&n, G, dep, k_sor_begin, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
-    dep = {n};
-    cudaGraph_t outer;
-    GK(add_while(&n, G, dep, hout, &outer));
-    dep = {n};
     ctx->resident = false;
     if (P.sor_path != NTCFD_SOR_STREAMING) {
         ctx->resident = plan_resident<Tc>(ctx);
@@ -322,27 +315,33 @@ int build_graph(ntcfd_ctx* ctx) {
             return fail(ctx, NTCFD_EINVAL, "the resident SOR kernel does not fit this grid on this device");
     }
     if (ctx->resident) {
-        std::vector<cudaGraphNode_t> od;
-        cudaGraphNode_t m;
+        // the resident kernel runs the whole solve (every correction cycle), so the
+        // solve is two plain nodes: the defect (which also starts the solve) and the kernel
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
-        GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
+        GK(add_kernel(&n, G, dep, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
                       (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, (cudaGraphConditionalHandle)0, 0,
-                      ctx->ring, (unsigned int*)ctx->bar));
-        od = {m};
-        GK(add_kernel_ex(&m, outer, od, resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid), dim3(kResNT),
+                      ctx->ring, (unsigned int*)ctx->bar, 1));
+        dep = {n};
+        GK(add_kernel_ex(&n, G, dep, resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid), dim3(kResNT),
                          ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, (const double*)ctx->b,
                          eR, eB, dR, dB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
                          ctx->bar, P.omega, P.zeta, P.itmax, ctx->cycle_len, ctx->csweeps, ctx->ring));
-        od = {m};
-        GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
+        dep = {n};
     } else {
+        cudaGraphConditionalHandle hout, hin;
+        GK(cudaGraphConditionalHandleCreate(&hout, G, 0, 0));
+        GK(add_kernel(&n, G, dep, k_sor_begin, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
+        dep = {n};
+        cudaGraph_t outer;
+        GK(add_while(&n, G, dep, hout, &outer));
+        dep = {n};
         GK(cudaGraphConditionalHandleCreate(&hin, outer, 0, 0));
         std::vector<cudaGraphNode_t> od;
         cudaGraphNode_t m;
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
         GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
                       (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, hin, 1,
-                      (unsigned long long*)nullptr, (unsigned int*)nullptr));
+                      (unsigned long long*)nullptr, (unsigned int*)nullptr, 0));
         od = {m};
         cudaGraph_t inner;
         GK(add_while(&m, outer, od, hin, &inner));
@@ -403,9 +402,11 @@ int build_graph(ntcfd_ctx* ctx) {
                       (const double*)ctx->v, (const double*)ctx->w, ctx->divslot));
         dep = {n};
     }
-    const int fixed = 10 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0);
+    // kernels of a step: predictor, rhs, project, force (2), bc (3), step_end, + LES, + diagnostic;
+    // + sor_begin and 3 per cycle (streaming) or 2 per solve (resident)
+    const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
+                  P.diag_divergence, fixed, ctx->resident ? 2 : 3, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
     GK(cudaGraphInstantiate(&ctx->exec, G, 0));
     return 0;
 }
@@ -423,7 +424,6 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-    k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
     Ctl& h = *hc;
     h = Ctl{};
     auto read_ctl = [&]() -> int {
@@ -431,21 +431,27 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         CK(cudaStreamSynchronize(st));
         return 0;
     };
+    if (ctx->resident) {
+        // one defect (starting the solve) and one launch that runs every cycle
+        k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, ctx->ring,
+                                        (unsigned int*)ctx->bar, 1);
+        void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&b, (void*)&eR,
+                        (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
+                        (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
+                        (void*)&itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
+        CK(cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
+                                       dim3(kResNT), args, ctx->res_smem, st));
+        if (int rc = read_ctl()) return rc;
+        CK(cudaGetLastError());
+        return 0;
+    }
+    k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
     bool more = itmax > 0;
     const int big_guard = ctx->csweeps > 1 ? 1 : 0;
     while (more) {
-        if (ctx->resident) {
-            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, ctx->ring,
-                                            (unsigned int*)ctx->bar);
-            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&b, (void*)&eR,
-                            (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
-                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
-                            (void*)&itmax, (void*)&ctx->cycle_len, (void*)&ctx->csweeps, (void*)&ctx->ring};
-            CK(cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
-                                           dim3(kResNT), args, ctx->res_smem, st));
-        } else {
+        {
             k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, nullptr,
-                                            nullptr);
+                                            nullptr, 0);
             const dim3 bs(kSweepBx, kSweepBy, 1);
             const int half = (g.nx + 1) / 2;
             const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
@@ -508,8 +514,8 @@ int run_step_eager(ntcfd_ctx* ctx) {
     k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
-    const int fixed = 10 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0);
-    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed,
+    const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
+    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed, ctx->resident ? 2 : 3,
                                 ctx->resident ? 0 : 2 * ctx->csweeps + 1);
     CK(cudaGetLastError());
     return 0;
@@ -618,7 +624,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
     if ((rc = timed([&] {
              k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
-                                                      ctx->ctl, 0, 0, nullptr, nullptr);
+                                                      ctx->ctl, 0, 0, nullptr, nullptr, 0);
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
@@ -642,7 +648,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
                            ctx->stream));
         if ((rc = timed([&] {
                  k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, pscratch, ctx->b, dR, dB, eR, eB,
-                                                          ctx->ctl, 0, 0, ctx->ring, (unsigned int*)ctx->bar);
+                                                          ctx->ctl, 0, 0, ctx->ring, (unsigned int*)ctx->bar, 0);
                  int zero = 0;
                  (void)zero;
                  cudaMemsetAsync(&ctx->ctl->ik, 0, sizeof(int), ctx->stream);
