@@ -51,11 +51,37 @@ struct PredArgs {
     long long fstride;   // N
 };
 
-// One thread per cell (i,j,k), i fastest.  Reads u,v,w (+-2 stencil) and
-// writes u*, v*, w* on the interior 1..nx, 1..ny, 1..nz (wall faces included,
-// as the reference does).
+// One thread per cell (i,j,k), i fastest, in blocks of kPredBX x kPredBY x
+// kPredBZ.  Reads u,v,w (+-2 stencil) and writes u*, v*, w* on the interior
+// 1..nx, 1..ny, 1..nz (wall faces included, as the reference does).  The
+// block's slices of the six metric tables of each axis (indices base-2 ..
+// base+extent+2) are staged in shared memory first.
+constexpr int kPredBX = 32, kPredBY = 4, kPredBZ = 2;
+
 template <class T>
-__global__ void __launch_bounds__(256) k_predictor(Geom g, Tabs<T> tb, PredArgs a) {
+__global__ void __launch_bounds__(kPredBX * kPredBY * kPredBZ) k_predictor(Geom g, Tabs<T> tb, PredArgs a) {
+    constexpr int LX = kPredBX + 5, LY = kPredBY + 5, LZ = kPredBZ + 5;
+    __shared__ T stx[6 * LX], sty[6 * LY], stz[6 * LZ];
+    const int tid = threadIdx.x + kPredBX * (threadIdx.y + kPredBY * threadIdx.z);
+    const int ib = blockIdx.x * kPredBX - 1, jb = blockIdx.y * kPredBY - 1, kb = blockIdx.z * kPredBZ - 1;
+    {
+        auto tab = [](const AxisTabs<T>& A, int t) {
+            return t == 0 ? A.riD : t == 1 ? A.rDs : t == 2 ? A.As : t == 3 ? A.Bs : t == 4 ? A.Ac : A.Bc;
+        };
+        for (int q = tid; q < 6 * (LX + LY + LZ); q += kPredBX * kPredBY * kPredBZ) {
+            if (q < 6 * LX) {
+                const int t = q / LX, o = q - t * LX;
+                if (ib + o <= g.nx + 2) stx[q] = tab(tb.ax[0], t)[ib + o];
+            } else if (q < 6 * (LX + LY)) {
+                const int r = q - 6 * LX, t = r / LY, o = r - t * LY;
+                if (jb + o <= g.ny + 2) sty[r] = tab(tb.ax[1], t)[jb + o];
+            } else {
+                const int r = q - 6 * (LX + LY), t = r / LZ, o = r - t * LZ;
+                if (kb + o <= g.nz + 2) stz[r] = tab(tb.ax[2], t)[kb + o];
+            }
+        }
+    }
+    __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -66,7 +92,13 @@ __global__ void __launch_bounds__(256) k_predictor(Geom g, Tabs<T> tb, PredArgs 
     const double* __restrict__ v = a.v;
     const double* __restrict__ w = a.w;
 #define LD(p, o) ((T)__ldg((p) + c + (o)))
-    const AxisTabs<T> X = tb.ax[0], Y = tb.ax[1], Z = tb.ax[2];
+    // the staged tables, indexed like the global ones (valid for the block's range)
+    const AxisTabs<T> X{stx - ib, stx + LX - ib, stx + 2 * LX - ib, stx + 3 * LX - ib, stx + 4 * LX - ib,
+                        stx + 5 * LX - ib};
+    const AxisTabs<T> Y{sty - jb, sty + LY - jb, sty + 2 * LY - jb, sty + 3 * LY - jb, sty + 4 * LY - jb,
+                        sty + 5 * LY - jb};
+    const AxisTabs<T> Z{stz - kb, stz + LZ - kb, stz + 2 * LZ - kb, stz + 3 * LZ - kb, stz + 4 * LZ - kb,
+                        stz + 5 * LZ - kb};
     const T dt = (T)a.dt;
     const T nue = (T)(a.les ? a.nu + __ldg(a.nut + c) * (double)a.les : a.nu);
 
