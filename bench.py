@@ -49,7 +49,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--n", type=int, default=128, help="cavity cells per side")
+    ap.add_argument("--n", type=int, default=None, help="cavity cells per side (default: the case's)")
+    ap.add_argument("--case", choices=("c2", "c1"), default="c2",
+                    help="c2: 128^3 cavity, Re=1000, dt=5e-4 (the headline); c1: 40^3, Re=100, dt=1e-3")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -62,7 +64,12 @@ def parse():
     ap.add_argument("--no-roofline", action="store_true", help="skip the standalone kernel timing")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost/accuracy leg")
     ap.add_argument("--no-fd", action="store_true", help="skip the finite-difference check of the adjoint")
-    return ap.parse_args()
+    a = ap.parse_args()
+    # the cavity of the case: Reynolds number, time step (a Fortran default-real literal) and size
+    a.Re, a.dt = (1000.0, 5e-4) if a.case == "c2" else (100.0, 1e-3)
+    if a.n is None:
+        a.n = 128 if a.case == "c2" else 40
+    return a
 
 
 # ------------------------------------------------------------------ ranks
@@ -149,7 +156,7 @@ class ClockSampler:
 # ------------------------------------------------------------------ our arm
 def cavity_case(n, precision, device, args):
     from ntustcfdlab_b200 import cases
-    c = cases.cavity(n, 1000.0, 5e-4, 500, precision=precision)
+    c = cases.cavity(n, args.Re, args.dt, 500, precision=precision)
     c.params.device = device
     c.params.mixed_cycle = args.cycle if precision == 1 else 0
     c.params.eager = 1 if args.eager else 0
@@ -440,7 +447,7 @@ def run_ours(args):
             "steps": K, "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic (lid-driven cavity from rest, no dataset)",
-            "config": {"workload": f"lid-driven cavity {args.n}^3, Re=1000, dt=5e-4, zeta=1e-4, "
+            "config": {"workload": f"lid-driven cavity {args.n}^3, Re={args.Re:g}, dt={args.dt:g}, zeta=1e-4, "
                                    f"mixed precision (FP32 red-black SOR + FP64 defect correction "
                                    f"every {args.cycle} sweeps)",
                        "sor_path": {1: "streaming", 2: "resident"}.get(path, str(path)),
@@ -474,7 +481,7 @@ def run_reference(args):
     from ntustcfdlab_b200.abi import SOR_LEX, params_copy
     from ntustcfdlab_b200 import cases
     from ntustcfdlab_b200.abi import MIXED
-    c = cases.cavity(args.n, 1000.0, 5e-4, 500, precision=MIXED)
+    c = cases.cavity(args.n, args.Re, args.dt, 500, precision=MIXED)
     threads = os.cpu_count() or 1
     o = cpu_oracle.Oracle(params_copy(c.params, sor_order=SOR_LEX), c.grid, threads=threads)
     o.initial_conditions()
@@ -498,7 +505,7 @@ def run_reference(args):
             "n_gpus": 0, "steps": done, "warmup": args.warmup, "ms_per_step": el * 1e3 / done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (lid-driven cavity from rest, no dataset)",
-            "config": {"workload": f"lid-driven cavity {args.n}^3, Re=1000, dt=5e-4, zeta=1e-4",
+            "config": {"workload": f"lid-driven cavity {args.n}^3, Re={args.Re:g}, dt={args.dt:g}, zeta=1e-4",
                        "grid": [args.n] * 3, "parallelism": f"{threads} OpenMP threads"},
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample},

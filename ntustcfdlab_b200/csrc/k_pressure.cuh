@@ -108,7 +108,8 @@ __global__ void k_make_rd(Geom g, SorCoef<Tc> sc, Tc* rdR, Tc* rdB) {
     else rdB[q] = rd;
 }
 
-// One half-sweep over colour `colour` (0 = red, (i+j+k) even).  Thread t of
+// One half-sweep over colour `colour` (0 = red, (i+j+k) even), column form
+// (used for FP64 e).  Thread t of
 // row (j,k) owns the cell i = 2t + 2 - r, m = t + 2 - r, r = ((j+k)^colour)&1,
 // for KPT consecutive planes k; all loads of the KPT cells are issued before
 // any arithmetic so that a warp keeps 9*KPT loads in flight.  Offsets are
@@ -117,7 +118,7 @@ __global__ void k_make_rd(Geom g, SorCoef<Tc> sc, Tc* rdR, Tc* rdB) {
 // sweep budget (itmax, cycle length) is used up.  The block's max |change|
 // goes to slot sub*kSpread + (block index mod kSpread).
 template <class Tc, int NT, int KPT>
-__global__ void __launch_bounds__(NT) k_sweep(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
+__global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
                                               const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
                                               const Tc* __restrict__ rdOwn, int colour, double omega,
                                               const Ctl* ctl, int sub, int itmax, int cycle_len,
@@ -174,6 +175,83 @@ __global__ void __launch_bounds__(NT) k_sweep(Geom g, SorCoef<Tc> sc, Tc* __rest
     }
     const int blin = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_max_bits<NT>(ch, &slots[sub * kSpread + (blin & (kSpread - 1))]);
+}
+
+// One half-sweep over colour `colour` (0 = red, (i+j+k) even), row form (used
+// for FP32 e).  One warp per row (j,k), rows j-fastest so that the warps of a block share their j+-1
+// neighbour rows; the colour's cells of a row are contiguous in the
+// colour-split arrays (m = t + 2 - r, r = ((j+k)^colour)&1, i = 2t + 2 - r),
+// so the row's base offsets are formed once and each lane updates two cells
+// per step (t and t + 32) with every load issued before its stores.  With
+// guard = 1 (several sweeps per loop body) the sweep is skipped once the
+// sweep budget (itmax, cycle length) is used up.  The block's max |change|
+// goes to slot sub*kSpread + (block index mod kSpread).
+template <class Tc, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
+                                              const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
+                                              const Tc* __restrict__ rdOwn, int colour, double omega,
+                                              const Ctl* ctl, int sub, int itmax, int cycle_len,
+                                              int guard, unsigned long long* slots) {
+    if (guard) {
+        const int ik = ctl->ik, inner = ctl->inner;
+        if (ik + sub >= itmax || inner + sub >= cycle_len) return;
+    }
+    using B = decltype(abs_bits(Tc(0)));
+    const int lane = threadIdx.x & 31;
+    const int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+    B ch = B(0);   // max |change| as an order-preserving pattern (NaN stays on top)
+    if (row < g.ny * g.nz) {
+        const int j = row % g.ny + 1, k = row / g.ny + 1;
+        const int r = ((j + k) ^ colour) & 1;
+        const int ys = g.mxp;
+        const long long zs = g.mz;
+        const long long rb = (long long)ys * (j + 1) + zs * (k + 1);   // colour-split row, m = 0
+        const Tc* __restrict__ oC = eOth + rb;
+        const Tc* __restrict__ oN = oC + ys;
+        const Tc* __restrict__ oS = oC - ys;
+        const Tc* __restrict__ oF = oC + zs;
+        const Tc* __restrict__ oB = oC - zs;
+        Tc* __restrict__ eR = eOwn + rb;
+        const Tc* __restrict__ dR = dOwn + rb;
+        const Tc* __restrict__ rR = rdOwn + rb;
+        const Tc cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
+        const Tc om = (Tc)omega;
+        const int half = (g.nx + 1) / 2;
+        for (int tA = lane; tA < half; tA += 64) {
+            const int iA = 2 * tA + 2 - r;
+            if (iA > g.nx) break;
+            const int tB = tA + 32;
+            const int iB0 = 2 * tB + 2 - r;
+            const bool okB = tB < half && iB0 <= g.nx;
+            const int mA = tA + 2 - r, mB = okB ? tB + 2 - r : mA;
+            const int iB = okB ? iB0 : iA;
+            const Tc eA = sc.cE[iA], wA = sc.cW[iA], eB = sc.cE[iB], wB = sc.cW[iB];
+            const Tc nEA = oC[mA + r], nWA = oC[mA - 1 + r], nNA = oN[mA], nSA = oS[mA], nFA = oF[mA],
+                     nBA = oB[mA];
+            const Tc nEB = oC[mB + r], nWB = oC[mB - 1 + r], nNB = oN[mB], nSB = oS[mB], nFB = oF[mB],
+                     nBB = oB[mB];
+            const Tc dA = dR[mA], dB_ = dR[mB], e0A = eR[mA], e0B = eR[mB], rdA = rR[mA], rdB = rR[mB];
+            const Tc sA = eA * nEA + wA * nWA + cN * nNA + cS * nSA + cF * nFA + cB * nBA;
+            const Tc sB = eB * nEB + wB * nWB + cN * nNB + cS * nSB + cF * nFB + cB * nBB;
+            const Tc diffA = (rdA * sA + dA) - e0A;
+            const Tc diffB = (rdB * sB + dB_) - e0B;
+            eR[mA] = e0A + om * diffA;
+            const B dbA = abs_bits(diffA);
+            ch = dbA > ch ? dbA : ch;
+            if (okB) {
+                eR[mB] = e0B + om * diffB;
+                const B dbB = abs_bits(diffB);
+                ch = dbB > ch ? dbB : ch;
+            }
+        }
+    }
+    block_max_bits<NT>(ch, &slots[sub * kSpread + (blockIdx.x & (kSpread - 1))]);
+}
+
+// Launch shape of k_sweep_rows: NT threads, one warp per row.
+inline dim3 sweep_grid(const Geom& g, int nt) {
+    const long long rows = (long long)g.ny * g.nz;
+    return dim3((unsigned)((rows + nt / 32 - 1) / (nt / 32)));
 }
 
 // One warp: the max over the kSpread slots of that sweep is its max|change|.

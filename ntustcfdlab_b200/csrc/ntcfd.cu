@@ -34,12 +34,36 @@ using namespace ntcfd;
 namespace {
 
 constexpr int kProjKc = 8;      // planes per column chunk in K4
-constexpr int kSweepBx = 64;    // threads per row in a half-sweep
+constexpr int kSweepNT = 256;    // threads per CTA of a streaming half-sweep
+constexpr int kSweepBx = 64;     // column form: threads per row, rows per CTA, planes per thread
 constexpr int kSweepBy = 4;
-constexpr int kSweepKpt = 4;     // planes per thread in a half-sweep
+constexpr int kSweepKpt = 4;
 constexpr int kResNT = 512;      // threads per CTA of the resident SOR kernel
 const double kZeroZeta = 0.0;
 const int kOne = 1;
+
+// The streaming half-sweep of a precision.  FP64 moves 40 B per cell and runs
+// closest to the HBM bandwidth in the column form (four planes per thread,
+// 36 loads in flight); FP32 is instruction-bound in that form and faster with
+// one warp per row.  Both do the same arithmetic per cell.
+template <class Tc>
+struct Sweep;
+template <>
+struct Sweep<double> {
+    static constexpr auto fn = k_sweep_cols<double, kSweepBx * kSweepBy, kSweepKpt>;
+    static dim3 block() { return dim3(kSweepBx, kSweepBy, 1); }
+    static dim3 grid(const Geom& g) {
+        const int half = (g.nx + 1) / 2;
+        return dim3((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
+                    (g.nz + kSweepKpt - 1) / kSweepKpt);
+    }
+};
+template <>
+struct Sweep<float> {
+    static constexpr auto fn = k_sweep_rows<float, kSweepNT>;
+    static dim3 block() { return dim3(kSweepNT); }
+    static dim3 grid(const Geom& g) { return sweep_grid(g, kSweepNT); }
+};
 
 struct DevTabs {
     // one allocation per precision; every table has n+5 entries (index -2..n+2)
@@ -350,18 +374,15 @@ int build_graph(ntcfd_ctx* ctx) {
             std::vector<cudaGraphNode_t> id;
             cudaGraphNode_t s;
             const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-            const dim3 bs(kSweepBx, kSweepBy, 1);
-            const int half = (g.nx + 1) / 2;
-            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
-                          (g.nz + kSweepKpt - 1) / kSweepKpt);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
             const Ctl* cctl = ctx->ctl;
             for (int sub = 0; sub < ctx->csweeps; ++sub) {
-                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt>, gs, bs, g, sc,
+                GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eR, (const Tc*)eB, (const Tc*)dR, (const Tc*)ctx->rdR, 0, P.omega, cctl,
                               sub, P.itmax,
                               ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
                 id = {s};
-                GK(add_kernel(&s, inner, id, k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt>, gs, bs, g, sc,
+                GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eB, (const Tc*)eR, (const Tc*)dB, (const Tc*)ctx->rdB, 1, P.omega, cctl,
                               sub, P.itmax,
                               ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
@@ -452,16 +473,13 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         {
             k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, nullptr,
                                             nullptr, 0);
-            const dim3 bs(kSweepBx, kSweepBy, 1);
-            const int half = (g.nx + 1) / 2;
-            const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
-                          (g.nz + kSweepKpt - 1) / kSweepKpt);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
-                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                    Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
                         ctx->cycle_len, big_guard, ctx->slots);
-                    k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, st>>>(
+                    Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
                         ctx->cycle_len, big_guard, ctx->slots);
                 }
@@ -628,15 +646,12 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-    const dim3 bs(kSweepBx, kSweepBy, 1);
-    const int half = (g.nx + 1) / 2;
-    const dim3 gs((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
-                  (g.nz + kSweepKpt - 1) / kSweepKpt);
+    const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
     const int big = 1 << 30;
     if ((rc = timed([&] {
-             k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, ctx->stream>>>(
+             Sweep<Tc>::fn<<<gs, bs, 0, ctx->stream>>>(
                  g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
-             k_sweep<Tc, kSweepBx * kSweepBy, kSweepKpt><<<gs, bs, 0, ctx->stream>>>(
+             Sweep<Tc>::fn<<<gs, bs, 0, ctx->stream>>>(
                  g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
          }, &out->sweep_ms, 2)))
         return rc;
