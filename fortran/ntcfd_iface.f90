@@ -241,5 +241,30 @@ module ntcfd_iface
          integer(c_int), value :: npts
          real(c_double), intent(out) :: z(*), y(*)
       end function
+
+      integer(c_int) function ntcfd_write_plot3d_x(path, nx, ny, nz, X, Y, Z) &
+            bind(C, name="ntcfd_write_plot3d_x")
+         import :: c_int, c_double, c_char
+         character(kind=c_char), intent(in) :: path(*)      ! NUL-terminated
+         integer(c_int), value :: nx, ny, nz
+         real(c_double), intent(in) :: X(*), Y(*), Z(*)
+      end function
+
+      integer(c_int) function ntcfd_write_plot3d_q(path, nx, ny, nz, pre, uc, vc, wc, eta, append) &
+            bind(C, name="ntcfd_write_plot3d_q")
+         import :: c_int, c_double, c_char
+         character(kind=c_char), intent(in) :: path(*)
+         integer(c_int), value :: nx, ny, nz
+         real(c_double), intent(in) :: pre(*), uc(*), vc(*), wc(*), eta(*)
+         integer(c_int), value :: append
+      end function
+
+      integer(c_int) function ntcfd_read_plot3d_q(path, nx, ny, nz, u, v, w, p) &
+            bind(C, name="ntcfd_read_plot3d_q")
+         import :: c_int, c_double, c_char
+         character(kind=c_char), intent(in) :: path(*)
+         integer(c_int), value :: nx, ny, nz
+         real(c_double), intent(inout) :: u(*), v(*), w(*), p(*)
+      end function
    end interface
 end module ntcfd_iface

@@ -50,6 +50,34 @@ int ntcfd_naca4_polygon_te(double t, int npts, int closed_te, double* z, double*
  * counter-clockwise from angle 0, last point = first point; returns npts+1. */
 int ntcfd_circle_polygon(double r, int npts, double* z, double* y);
 
+/* PLOT3D files in the reference's format: Fortran unformatted sequential
+ * records (4-byte length before and after each), default reals (4 bytes),
+ * one block.  Return 0, -1 for bad arguments, -2 for a file error, -3 for a
+ * file whose records do not match nx, ny, nz.
+ *
+ * ntcfd_write_plot3d_x: mesh.x of gridder.f90:150-212 -- the cell-centre
+ * coordinates (X(i) + X(i+1))/2 etc. from the node coordinates X, Y, Z (n+5
+ * entries, index -1..n+3, as ntcfd_gridder_* returns them). */
+int ntcfd_write_plot3d_x(const char* path, int nx, int ny, int nz,
+                         const double* X, const double* Y, const double* Z);
+
+/* NNNN.q of filereachtime (filer.f90:161-187): pre, uc, vc, wc ((nx,ny,nz),
+ * as ntcfd_get_output returns them) and ETA (the halo array of
+ * ntcfd_get_mask, interior taken), with the four header reals 1.0.
+ * append = 1 adds the solution to the end of an existing file, as the
+ * reference's position='append' does; 0 replaces the file. */
+int ntcfd_write_plot3d_q(const char* path, int nx, int ny, int nz, const double* pre,
+                         const double* uc, const double* vc, const double* wc,
+                         const double* eta, int append);
+
+/* reading_variables (reading_data.f90:62-90): restart from the first
+ * solution of a .q file.  u, v, w, p are halo arrays ((n+4)^3); u(i,j,k) =
+ * 0.5 (uc(i) + uc(i+1)) in default-real arithmetic for i, j, k = 1..n-1 (and
+ * likewise v, w), p = pre on the interior; every other entry keeps the
+ * value the caller put there. */
+int ntcfd_read_plot3d_q(const char* path, int nx, int ny, int nz,
+                        double* u, double* v, double* w, double* p);
+
 #ifdef __cplusplus
 }
 #endif

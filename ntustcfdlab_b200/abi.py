@@ -187,6 +187,9 @@ SIGNATURES = {
     "ntcfd_naca4_polygon": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, _DP, _DP]),
     "ntcfd_naca4_polygon_te": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, ctypes.c_int, _DP, _DP]),
     "ntcfd_circle_polygon": (ctypes.c_int, [ctypes.c_double, ctypes.c_int, _DP, _DP]),
+    "ntcfd_write_plot3d_x": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_DP] * 3),
+    "ntcfd_write_plot3d_q": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_DP] * 5 + [ctypes.c_int]),
+    "ntcfd_read_plot3d_q": (ctypes.c_int, [ctypes.c_char_p] + [ctypes.c_int] * 3 + [_DP] * 4),
 }
 
 _lib = None

@@ -1,7 +1,8 @@
 """Builds ``ntustcfdlab_b200/lib/libntcfd.so`` in-tree for sm_100a.
 
 ``python -m ntustcfdlab_b200.build`` compiles the CUDA kernels and the C-ABI
-(``csrc/ntcfd.cu``) and the host set-up code (``csrc/host_grid.cpp``) with
+(``csrc/ntcfd.cu``), the host set-up code (``csrc/host_grid.cpp``) and the
+PLOT3D file I/O (``csrc/host_io.cpp``) with
 nvcc for ``-gencode arch=compute_100a,code=sm_100a``.  nvcc cross-compiles,
 so the build needs no GPU.
 """
@@ -16,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 OUT = os.path.join(LIB_DIR, "libntcfd.so")
-SOURCES = ["ntcfd.cu", "host_grid.cpp"]
+SOURCES = ["ntcfd.cu", "host_grid.cpp", "host_io.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

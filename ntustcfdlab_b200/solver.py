@@ -75,6 +75,41 @@ def circle_polygon(r: float, npts: int = 128):
     return z[:n], y[:n]
 
 
+def write_plot3d_x(path: str, grid: dict):
+    """mesh.x of gridder.f90:150-212 (cell-centre coordinates, default reals)."""
+    lib = abi.load_library()
+    nx, ny, nz = len(grid["X"]) - 5, len(grid["Y"]) - 5, len(grid["Z"]) - 5
+    X, Y, Z = (np.ascontiguousarray(grid[k], dtype=np.float64) for k in "XYZ")
+    rc = lib.ntcfd_write_plot3d_x(path.encode(), nx, ny, nz, dptr(X), dptr(Y), dptr(Z))
+    if rc:
+        raise OSError(f"ntcfd_write_plot3d_x({path!r}) returned {rc}")
+
+
+def write_plot3d_q(path: str, pre, uc, vc, wc, eta, append: bool = True):
+    """One NNNN.q solution of filereachtime (filer.f90:161-187): pre, uc, vc, wc
+    ((nx, ny, nz)) and the interior of the halo array ETA, appended by default
+    as the reference does."""
+    lib = abi.load_library()
+    nx, ny, nz = pre.shape
+    arrs = [np.asfortranarray(a, dtype=np.float64) for a in (pre, uc, vc, wc, eta)]
+    rc = lib.ntcfd_write_plot3d_q(path.encode(), nx, ny, nz, *[dptr(a) for a in arrs], 1 if append else 0)
+    if rc:
+        raise OSError(f"ntcfd_write_plot3d_q({path!r}) returned {rc}")
+
+
+def read_plot3d_q(path: str, u, v, w, p):
+    """reading_variables (reading_data.f90:62-90): fills the halo arrays u, v,
+    w, p (Fortran-ordered float64, modified in place) from a .q file."""
+    lib = abi.load_library()
+    nx, ny, nz = (d - 4 for d in u.shape)
+    for a in (u, v, w, p):
+        if a.dtype != np.float64 or not a.flags["F_CONTIGUOUS"]:
+            raise TypeError("halo arrays must be Fortran-ordered float64")
+    rc = lib.ntcfd_read_plot3d_q(path.encode(), nx, ny, nz, dptr(u), dptr(v), dptr(w), dptr(p))
+    if rc:
+        raise OSError(f"ntcfd_read_plot3d_q({path!r}) returned {rc}")
+
+
 class Solver:
     """One device-resident grid (an ``ntcfd_ctx``)."""
 
