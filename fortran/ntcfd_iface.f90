@@ -40,6 +40,7 @@ module ntcfd_iface
       integer(c_int) :: sor_iters, converged
       real(c_double) :: sor_last_change, cDrag, cLift, div_max
       integer(c_int) :: dc_cycles, launches, sor_path, pad
+      real(c_double) :: aoa
    end type ntcfd_step_info
 
    type, bind(C) :: ntcfd_kernel_times
@@ -184,6 +185,27 @@ module ntcfd_iface
          type(c_ptr), value :: ctx
          integer(c_int), value :: reps
          type(ntcfd_kernel_times), intent(out) :: times
+      end function
+
+      integer(c_int) function ntcfd_set_dynamic_aoa(ctx, az, ay, npts, aoa1, reduce_frequency, zc, yc, &
+            start_step) bind(C, name="ntcfd_set_dynamic_aoa")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: az(*), ay(*)
+         integer(c_int), value :: npts
+         real(c_double), value :: aoa1, reduce_frequency, zc, yc
+         integer(c_int), value :: start_step
+      end function
+
+      integer(c_int) function ntcfd_output_async(ctx) bind(C, name="ntcfd_output_async")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+      end function
+
+      integer(c_int) function ntcfd_output_wait(ctx, pre, uc, vc, wc) bind(C, name="ntcfd_output_wait")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: pre(*), uc(*), vc(*), wc(*)
       end function
 
       ! fu, fv, fw: c_loc of an (nx,ny,nz) array, or c_null_ptr for a zero component

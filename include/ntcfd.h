@@ -99,6 +99,7 @@ typedef struct ntcfd_step_info {
     int launches;            /* device kernels launched for this step */
     int sor_path;            /* NTCFD_SOR_STREAMING or NTCFD_SOR_RESIDENT: the path that ran */
     int pad;
+    double aoa;              /* angle of attack of the step's mask under ntcfd_set_dynamic_aoa, else 0 */
 } ntcfd_step_info;
 
 /* Average device time of single kernels of the step, for the roofline. */
@@ -202,6 +203,33 @@ int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms);
  * stream with CUDA events and returns the averages.  The velocity, pressure
  * and ETA of the context are left unchanged. */
 int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
+
+/* dynamic_AOA + RayCasting inside the time loop (airfoil.f90:311-321,
+ * main.f90:144-155).  From the context's step start_step on (steps counted
+ * from 1 over every ntcfd_step call), each step first sets
+ *     AOA = aoa1 + 10 |sin(2 pi f (time - dt (start_step - 1)))|,
+ *     f = reduce_frequency / pi,
+ * with time the simulated time before the step and pi the reference's
+ * default-real literal 3.14159265359, and rebuilds ETA by ray casting the
+ * polygon (az, ay) at that angle about (zc, yc) as ntcfd_build_mask_polygon
+ * does, through the allocation-free variant (so the limits of
+ * ntcfd_build_mask_polygon_noalloc apply, checked here).  The angle used is
+ * reported in ntcfd_step_info.aoa.  A step whose polygon meets an exact
+ * vertex/grid tie stops the call with NTCFD_EINVAL (the reference moves the
+ * grid instead).  npts = 0 switches the dynamic angle off. */
+int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
+                          double aoa1, double reduce_frequency, double zc, double yc,
+                          int start_step);
+
+/* The centred output of ntcfd_get_output without waiting for it: the fields
+ * of the last completed step are formed on the context's stream and copied
+ * to a context-owned pinned host buffer on a second stream, so that the
+ * following ntcfd_step calls overlap the copy (filereachtime every isto
+ * steps, main.f90:318-324).  ntcfd_output_wait blocks until that copy is
+ * done and copies the fields out (any pointer may be NULL).  One output is
+ * in flight at a time: ntcfd_output_async first waits for the previous one. */
+int ntcfd_output_async(ntcfd_ctx* ctx);
+int ntcfd_output_wait(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc);
 
 /* ------------------------------------------------------------------------
  * Body force and discrete adjoint.  No counterpart in the reference: its

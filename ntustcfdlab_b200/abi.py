@@ -68,6 +68,7 @@ class NtcfdStepInfo(ctypes.Structure):
         ("div_max", ctypes.c_double),
         ("dc_cycles", ctypes.c_int), ("launches", ctypes.c_int),
         ("sor_path", ctypes.c_int), ("pad", ctypes.c_int),
+        ("aoa", ctypes.c_double),
     ]
 
 
@@ -178,6 +179,10 @@ SIGNATURES = {
     "ntcfd_time_kernels": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int,
                                           ctypes.POINTER(NtcfdKernelTimes)]),
     "ntcfd_set_body_force": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 3),
+    "ntcfd_set_dynamic_aoa": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int] + [ctypes.c_double] * 4
+                              + [ctypes.c_int]),
+    "ntcfd_output_async": (ctypes.c_int, [ctypes.c_void_p]),
+    "ntcfd_output_wait": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),
     "ntcfd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NtcfdAdjSpec),
                                      ctypes.POINTER(NtcfdAdjResult), _DP, _DP, _DP,
                                      ctypes.POINTER(NtcfdStepInfo)]),

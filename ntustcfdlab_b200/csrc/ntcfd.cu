@@ -121,6 +121,17 @@ struct ntcfd_ctx {
     std::vector<void*> allocs;
     void* adj_buf = nullptr;                // ntcfd_adjoint workspace, kept between calls
     size_t adj_cap = 0;
+    long long istep = 0;                    // steps taken by ntcfd_step since ntcfd_create
+    // dynamic angle of attack (ntcfd_set_dynamic_aoa); dyn_start = 0: off
+    std::vector<double> dyn_az, dyn_ay;
+    double dyn_aoa1 = 0.0, dyn_rf = 0.0, dyn_zc = 0.0, dyn_yc = 0.0;
+    int dyn_start = 0;
+    // asynchronous output (ntcfd_output_async)
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t out_ready = nullptr, out_done = nullptr;
+    double* out_dev = nullptr;              // pre, uc, vc, wc on the device
+    double* out_host = nullptr;             // pinned copy
+    bool out_pending = false;
 };
 
 namespace {
@@ -827,6 +838,11 @@ void ntcfd_destroy(ntcfd_ctx* ctx) {
     for (void* q : ctx->allocs) cudaFree(q);
     if (ctx->rec) cudaFree(ctx->rec);
     if (ctx->adj_buf) cudaFree(ctx->adj_buf);
+    if (ctx->out_stream) cudaStreamSynchronize(ctx->out_stream);
+    if (ctx->out_host) cudaFreeHost(ctx->out_host);
+    if (ctx->out_ready) cudaEventDestroy(ctx->out_ready);
+    if (ctx->out_done) cudaEventDestroy(ctx->out_done);
+    if (ctx->out_stream) cudaStreamDestroy(ctx->out_stream);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1023,7 +1039,14 @@ int ntcfd_get_output(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double
 
 }  // extern "C"
 
+extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az_in, const double* ay_in,
+                                                int npts, double aoa, double zc, double yc, int* ties_out);
+
 namespace {
+
+// Limits of the allocation-free mask scratch (defined with the scratch below).
+constexpr int kNaPoly = 16384;      // polygon points
+constexpr int kNaCells = 262144;    // ny * nz
 
 // Record buffer of at least nrec steps and an instantiated step graph (the
 // graph is built in eager mode too: it plans the SOR path).
@@ -1056,7 +1079,8 @@ int launch_step(ntcfd_ctx* ctx) {
 
 // Advances the simulated time by one dt per record, fills `info` (may be
 // NULL) and returns the worst status of the records.
-int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_info* info) {
+int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_info* info,
+                    const double* aoa = nullptr) {
     int status = 0;
     for (int s = 0; s < nsteps; ++s) {
         ctx->time = ctx->time + ctx->prm.dt;   // main.f90:271
@@ -1075,6 +1099,7 @@ int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_i
             I.dc_cycles = rec[s].cycles;
             I.launches = rec[s].launches;
             I.sor_path = ctx->resident ? NTCFD_SOR_RESIDENT : NTCFD_SOR_STREAMING;
+            I.aoa = aoa ? aoa[s] : 0.0;
         }
     }
     if (status == NTCFD_ETIMEOUT) fail(ctx, status, "the resident SOR kernel's grid barrier gave up waiting");
@@ -1095,14 +1120,103 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     if (int rc = prepare_steps(ctx, nsteps)) return rc;
     CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (int s = 0; s < nsteps; ++s)
+    std::vector<double> aoa(nsteps, 0.0);
+    double t = ctx->time;
+    for (int s = 0; s < nsteps; ++s) {
+        const long long istep = ctx->istep + s + 1;
+        if (ctx->dyn_start > 0 && istep >= ctx->dyn_start) {
+            // dynamic_AOA (airfoil.f90:313-317): PI is the default-real literal 3.14159265359
+            const double PI = (double)3.14159265359f;
+            const double frequency = ctx->dyn_rf / PI;
+            aoa[s] = ctx->dyn_aoa1 +
+                     10 * std::fabs(std::sin(2 * PI * frequency * (t - ctx->prm.dt * (double)(ctx->dyn_start - 1))));
+            int ties = 0;
+            const int rc = ntcfd_build_mask_polygon_noalloc(ctx, ctx->dyn_az.data(), ctx->dyn_ay.data(),
+                                                            (int)ctx->dyn_az.size(), aoa[s], ctx->dyn_zc,
+                                                            ctx->dyn_yc, &ties);
+            if (rc) return rc;
+        }
         if (int rc = launch_step(ctx)) return rc;
+        t = t + ctx->prm.dt;
+    }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     std::vector<StepRec> rec(nsteps);
     CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
-    return records_to_info(ctx, rec.data(), nsteps, info);
+    ctx->istep += nsteps;
+    return records_to_info(ctx, rec.data(), nsteps, info, aoa.data());
+}
+
+int ntcfd_output_async(ntcfd_ctx* ctx) {
+    DEV();
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "metrics not set");
+    const Geom& g = ctx->g;
+    const size_t n = (size_t)g.nx * g.ny * g.nz;
+    if (!ctx->out_dev) {
+        double* q = nullptr;
+        if (int rc = dalloc(ctx, &q, 4 * n)) return rc;
+        ctx->out_dev = q;
+        CK(cudaMallocHost(&ctx->out_host, 4 * n * sizeof(double)));
+        CK(cudaStreamCreateWithFlags(&ctx->out_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->out_ready, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->out_done, cudaEventDisableTiming));
+    }
+    if (ctx->out_pending) {   // one copy in flight: the buffers are reused
+        CK(cudaEventSynchronize(ctx->out_done));
+        ctx->out_pending = false;
+    }
+    double* o = ctx->out_dev;
+    const dim3 b3(32, 4, 2);
+    k_centre<<<grid3(g, b3), b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->p, ctx->faceW,
+                                                   ctx->faceE, ctx->faceS, ctx->faceN, ctx->faceB,
+                                                   ctx->faceF, o, o + n, o + 2 * n, o + 3 * n);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->out_ready, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->out_stream, ctx->out_ready, 0));
+    CK(cudaMemcpyAsync(ctx->out_host, o, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->out_stream));
+    CK(cudaEventRecord(ctx->out_done, ctx->out_stream));
+    ctx->out_pending = true;
+    return 0;
+}
+
+int ntcfd_output_wait(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
+    DEV();
+    if (!ctx->out_pending) return fail(ctx, NTCFD_ESTATE, "no ntcfd_output_async in flight");
+    CK(cudaEventSynchronize(ctx->out_done));
+    ctx->out_pending = false;
+    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
+    double* dst[4] = {pre, uc, vc, wc};
+    for (int q = 0; q < 4; ++q)
+        if (dst[q]) std::memcpy(dst[q], ctx->out_host + q * n, n * sizeof(double));
+    return 0;
+}
+
+int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, int npts, double aoa1,
+                          double reduce_frequency, double zc, double yc, int start_step) {
+    DEV();
+    if (npts == 0) {
+        ctx->dyn_start = 0;
+        ctx->dyn_az.clear();
+        ctx->dyn_ay.clear();
+        return 0;
+    }
+    if (!az || !ay || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
+    if (start_step < 1) return fail(ctx, NTCFD_EINVAL, "start_step must be >= 1");
+    if (!std::isfinite(aoa1) || !std::isfinite(reduce_frequency) || !std::isfinite(zc) || !std::isfinite(yc))
+        return fail(ctx, NTCFD_EINVAL, "non-finite dynamic angle parameters");
+    if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    if (npts > kNaPoly || (size_t)ctx->g.ny * ctx->g.nz > (size_t)kNaCells)
+        return fail(ctx, NTCFD_EINVAL, "the dynamic angle rebuilds the mask without allocating: at most %d "
+                    "polygon points and %d cells in the (k,j) plane", kNaPoly, kNaCells);
+    ctx->dyn_az.assign(az, az + npts);
+    ctx->dyn_ay.assign(ay, ay + npts);
+    ctx->dyn_aoa1 = aoa1;
+    ctx->dyn_rf = reduce_frequency;
+    ctx->dyn_zc = zc;
+    ctx->dyn_yc = yc;
+    ctx->dyn_start = start_step;
+    return 0;
 }
 
 int ntcfd_last_step_ms(const ntcfd_ctx* ctx, float* ms) {
@@ -1224,8 +1338,6 @@ int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* 
 // device that loads the library.  Layout: az[kNaPoly], ay[kNaPoly] (double),
 // points[kNaCells], list[kNaCells] (int), the tie counter (int).
 namespace {
-constexpr int kNaPoly = 16384;
-constexpr int kNaCells = 1 << 18;
 constexpr size_t kNaPointsOff = 2 * sizeof(double) * (size_t)kNaPoly;
 constexpr size_t kNaListOff = kNaPointsOff + sizeof(int) * (size_t)kNaCells;
 constexpr size_t kNaTiesOff = kNaListOff + sizeof(int) * (size_t)kNaCells;
@@ -1701,6 +1813,8 @@ extern "C" int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_a
     std::memset(result, 0, sizeof *result);
     if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_adjoint");
     if (spec->nsteps < 1) return fail(ctx, NTCFD_EINVAL, "nsteps must be >= 1");
+    if (ctx->dyn_start > 0)
+        return fail(ctx, NTCFD_EINVAL, "the adjoint holds ETA fixed: switch the dynamic angle of attack off");
     if (spec->checkpoint_every < 1) return fail(ctx, NTCFD_EINVAL, "checkpoint_every must be >= 1");
     if (!(spec->adj_zeta >= 0.0) || spec->adj_itmax < 0) return fail(ctx, NTCFD_EINVAL, "bad adjoint stop rule");
     if (!(spec->adj_omega >= 0.0 && spec->adj_omega < 2.0))

@@ -217,6 +217,28 @@ class Solver:
         self._check(self.lib.ntcfd_get_output(self.h, *[dptr(a) for a in arrs]))
         return tuple(arrs)
 
+    def set_dynamic_aoa(self, az, ay, aoa1: float, reduce_frequency: float, zc: float, yc: float,
+                        start_step: int):
+        """dynamic_AOA + RayCasting before every step from start_step on
+        (airfoil.f90:311-321, main.f90:144-155); az=None switches it off."""
+        if az is None:
+            self._check(self.lib.ntcfd_set_dynamic_aoa(self.h, None, None, 0, 0.0, 0.0, 0.0, 0.0, 0))
+            return
+        az = np.ascontiguousarray(az, dtype=np.float64)
+        ay = np.ascontiguousarray(ay, dtype=np.float64)
+        self._check(self.lib.ntcfd_set_dynamic_aoa(self.h, dptr(az), dptr(ay), len(az), aoa1, reduce_frequency,
+                                                   zc, yc, start_step))
+
+    def output_async(self):
+        """Start the centred output of the last step without waiting for it."""
+        self._check(self.lib.ntcfd_output_async(self.h))
+
+    def output_wait(self):
+        """(pre, uc, vc, wc) of the last output_async."""
+        arrs = [np.zeros(self.inner_shape, dtype=np.float64, order="F") for _ in range(4)]
+        self._check(self.lib.ntcfd_output_wait(self.h, *[dptr(a) for a in arrs]))
+        return tuple(arrs)
+
     def step(self, nsteps: int = 1):
         """Runs the loop body nsteps times; returns (list of NtcfdStepInfo, status).
         status is 0 or NTCFD_NOT_CONVERGED; errors raise."""

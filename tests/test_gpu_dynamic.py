@@ -1,0 +1,108 @@
+"""Dynamic angle of attack (dynamic_AOA + RayCasting every step,
+airfoil.f90:311-321, main.f90:144-155) against the oracle stepping with the
+same angles, and the asynchronous centred output."""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import interior, rel_l2
+from ntustcfdlab_b200.abi import f4, make_params, params_copy
+
+pytestmark = pytest.mark.gpu
+
+N = (4, 48, 64)
+L = (1.0, 3.0, 4.0)
+BAND = (f4(12.5), 1.5, 1.2, 4, 20, 30, 24, 36, 1.0, f4(0.3), f4(0.6), f4(1.1), 2.0)
+AOA1, RF, ZC, YC, START, STEPS = 5.0, 2.0, 1.2, 1.5, 2, 4
+
+
+def params():
+    bc = {"West": ("periodic",) * 3, "East": ("periodic",) * 3,
+          "South": ("Neumann",) * 3, "North": ("Neumann",) * 3,
+          "Back": ("Dirichlet", "Dirichlet", "Dirichlet"), "Front": ("Neumann",) * 3}
+    return make_params(*N, Re=1000.0, dt=f4(1e-3), bc=bc, bc_value={"Back": (0.0, 0.0, 1.0)}, lx=L[0])
+
+
+def dynamic_aoa(t, dt):
+    # airfoil.f90:313-317 with the default-real PI literal
+    pi = float(np.float32(3.14159265359))
+    frequency = RF / pi
+    return AOA1 + 10 * abs(math.sin(2 * pi * frequency * (t - dt * (START - 1))))
+
+
+def test_dynamic_angle_matches_oracle(orc):
+    from ntustcfdlab_b200.solver import Solver, gridder_unequal, naca4_polygon
+    z, y = naca4_polygon(0.12, 64)
+    grid = gridder_unequal(*N, *L, BAND)
+    p = params()
+    # device
+    s = Solver(p, grid)
+    try:
+        s.build_mask_polygon(z, y, AOA1, ZC, YC)          # main.f90:109-110
+        s.set_dynamic_aoa(z, y, AOA1, RF, ZC, YC, START)
+        s.boundary_conditions()
+        info, rc = s.step(STEPS)
+        state, eta = s.get_state(), s.get_mask()
+    finally:
+        s.close()
+    # oracle
+    og = orc.gridder_unequal(*N, *L, BAND)
+    o = orc.Oracle(p, og)
+    o.initial_conditions()
+    assert o.raycasting(z, y, AOA1, ZC, YC) == 0
+    o.boundary_conditions()
+    angles, oi = [], []
+    for istep in range(1, STEPS + 1):
+        a = 0.0
+        if istep >= START:
+            a = dynamic_aoa(o.time, p.dt)
+            assert o.raycasting(z, y, a, ZC, YC) == 0
+        angles.append(a)
+        oi += o.step(1)
+    assert [i.aoa for i in info] == angles
+    assert angles[-1] != angles[-2] != AOA1
+    assert np.array_equal(eta, o.get("ETA"))
+    assert [i.sor_iters for i in info] == [i.sor_iters for i in oi]
+    for k, a in zip("uvwp", state):
+        assert rel_l2(interior(a), interior(o.get(k))) <= 1e-12, k
+
+
+def test_adjoint_refuses_a_moving_mask():
+    from ntustcfdlab_b200.solver import NtcfdError, Solver, gridder_unequal, naca4_polygon
+    z, y = naca4_polygon(0.12, 64)
+    s = Solver(params(), gridder_unequal(*N, *L, BAND))
+    try:
+        s.set_dynamic_aoa(z, y, AOA1, RF, ZC, YC, START)
+        with pytest.raises(NtcfdError):
+            s.adjoint(2, 1)
+        s.set_dynamic_aoa(None, None, 0, 0, 0, 0, 0)       # off again
+        s.boundary_conditions()
+        s.step(1)
+    finally:
+        s.close()
+
+
+def test_async_output_equals_get_output():
+    from ntustcfdlab_b200 import cases
+    from ntustcfdlab_b200.solver import NtcfdError, Solver
+    c = cases.cavity(24, 100.0, 1e-3, 10)
+    s = Solver(c.params, c.grid)
+    try:
+        s.boundary_conditions()
+        with pytest.raises(NtcfdError):
+            s.output_wait()                                  # nothing in flight
+        s.step(3)
+        s.output_async()
+        ref = s.get_output()
+        s.step(2)                                            # overlaps the copy
+        got = s.output_wait()
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b)
+        s.output_async()
+        s.output_async()                                     # waits for the first
+        got2 = s.output_wait()
+        for a, b in zip(got2, s.get_output()):
+            assert np.array_equal(a, b)
+    finally:
+        s.close()
