@@ -199,7 +199,8 @@ def e2e_run(case, K, isto=100):
     initial state from pinned host memory, one ntcfd_step(ctx, 1, &info) per
     step (info back to the host every step, as the reference driver prints
     it), centred output fields to the host every `isto` steps
-    (filereachtime cadence, main.f90:317-324) and the final state."""
+    (filereachtime cadence, main.f90:317-324) through ntcfd_output_async, so
+    the copy overlaps the following steps, and the final state."""
     import torch
     from ntustcfdlab_b200.solver import Solver
     s = Solver(case.params, case.grid)
@@ -222,14 +223,20 @@ def e2e_run(case, K, isto=100):
     lib.ntcfd_apply_bc(h)
     h2d = 4 * n_halo * 8
     d2h = 0
+    pending = False
     for k in range(1, K + 1):
         rc = lib.ntcfd_step(h, 1, info)
         if rc < 0:
             raise RuntimeError(s._err())
         d2h += 40  # the step record (StepRec) crosses back every step
         if k % isto == 0:
-            lib.ntcfd_get_output(h, *[dptr(a) for a in outs])
+            if pending:
+                lib.ntcfd_output_wait(h, *[dptr(a) for a in outs])
+            lib.ntcfd_output_async(h)
+            pending = True
             d2h += 4 * n_in * 8
+    if pending:
+        lib.ntcfd_output_wait(h, *[dptr(a) for a in outs])
     lib.ntcfd_get_state(h, *[dptr(a) for a in back])
     d2h += 4 * n_halo * 8
     t1 = time.perf_counter()
