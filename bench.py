@@ -217,6 +217,8 @@ def e2e_run(case, K, isto=100):
     lib, h = s.lib, s.h
     from ntustcfdlab_b200.abi import NtcfdStepInfo
     info = NtcfdStepInfo()
+    lib.ntcfd_output_async(h, *[dptr(a) for a in outs])   # allocates the output buffers
+    lib.ntcfd_output_wait(h)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     lib.ntcfd_set_state(h, *[dptr(a) for a in state])
@@ -229,14 +231,13 @@ def e2e_run(case, K, isto=100):
         if rc < 0:
             raise RuntimeError(s._err())
         d2h += 40  # the step record (StepRec) crosses back every step
-        if k % isto == 0:
-            if pending:
-                lib.ntcfd_output_wait(h, *[dptr(a) for a in outs])
-            lib.ntcfd_output_async(h)
+        if k % isto == 0:           # waits for the previous output first
+            if lib.ntcfd_output_async(h, *[dptr(a) for a in outs]) != 0:
+                raise RuntimeError(s._err())
             pending = True
             d2h += 4 * n_in * 8
-    if pending:
-        lib.ntcfd_output_wait(h, *[dptr(a) for a in outs])
+    if pending and lib.ntcfd_output_wait(h) != 0:
+        raise RuntimeError(s._err())
     lib.ntcfd_get_state(h, *[dptr(a) for a in back])
     d2h += 4 * n_halo * 8
     t1 = time.perf_counter()

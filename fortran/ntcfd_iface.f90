@@ -197,15 +197,17 @@ module ntcfd_iface
          integer(c_int), value :: start_step
       end function
 
-      integer(c_int) function ntcfd_output_async(ctx) bind(C, name="ntcfd_output_async")
-         import :: c_int, c_ptr
-         type(c_ptr), value :: ctx
-      end function
-
-      integer(c_int) function ntcfd_output_wait(ctx, pre, uc, vc, wc) bind(C, name="ntcfd_output_wait")
+      ! pre, uc, vc, wc are written after the call returns, until
+      ! ntcfd_output_wait: hence ASYNCHRONOUS here and on the actual arrays
+      integer(c_int) function ntcfd_output_async(ctx, pre, uc, vc, wc) bind(C, name="ntcfd_output_async")
          import :: c_int, c_ptr, c_double
          type(c_ptr), value :: ctx
-         real(c_double), intent(out) :: pre(*), uc(*), vc(*), wc(*)
+         real(c_double), asynchronous :: pre(*), uc(*), vc(*), wc(*)
+      end function
+
+      integer(c_int) function ntcfd_output_wait(ctx) bind(C, name="ntcfd_output_wait")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
       end function
 
       ! fu, fv, fw: c_loc of an (nx,ny,nz) array, or c_null_ptr for a zero component

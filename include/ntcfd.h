@@ -221,15 +221,18 @@ int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, in
                           double aoa1, double reduce_frequency, double zc, double yc,
                           int start_step);
 
-/* The centred output of ntcfd_get_output without waiting for it: the fields
- * of the last completed step are formed on the context's stream and copied
- * to a context-owned pinned host buffer on a second stream, so that the
- * following ntcfd_step calls overlap the copy (filereachtime every isto
- * steps, main.f90:318-324).  ntcfd_output_wait blocks until that copy is
- * done and copies the fields out (any pointer may be NULL).  One output is
- * in flight at a time: ntcfd_output_async first waits for the previous one. */
-int ntcfd_output_async(ntcfd_ctx* ctx);
-int ntcfd_output_wait(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc);
+/* The centred output of ntcfd_get_output without waiting for it
+ * (filereachtime every isto steps, main.f90:318-324): the fields of the last
+ * completed step are formed on the context's stream and copied into pre, uc,
+ * vc, wc on a second stream while the following ntcfd_step calls run.  The
+ * arrays (any may be NULL) belong to the copy until ntcfd_output_wait
+ * returns: the caller neither reads nor frees them before that.  Pinned
+ * (page-locked) arrays are written by the copy engine directly; pageable
+ * ones through a context-owned pinned buffer and a stream callback, off the
+ * caller's thread.  One output is in flight at a time: ntcfd_output_async
+ * first waits for the previous one.  The first call allocates its buffers. */
+int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc);
+int ntcfd_output_wait(ntcfd_ctx* ctx);
 
 /* ------------------------------------------------------------------------
  * Body force and discrete adjoint.  No counterpart in the reference: its

@@ -181,8 +181,8 @@ SIGNATURES = {
     "ntcfd_set_body_force": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 3),
     "ntcfd_set_dynamic_aoa": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int] + [ctypes.c_double] * 4
                               + [ctypes.c_int]),
-    "ntcfd_output_async": (ctypes.c_int, [ctypes.c_void_p]),
-    "ntcfd_output_wait": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),
+    "ntcfd_output_async": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),
+    "ntcfd_output_wait": (ctypes.c_int, [ctypes.c_void_p]),
     "ntcfd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NtcfdAdjSpec),
                                      ctypes.POINTER(NtcfdAdjResult), _DP, _DP, _DP,
                                      ctypes.POINTER(NtcfdStepInfo)]),

@@ -130,7 +130,10 @@ struct ntcfd_ctx {
     cudaStream_t out_stream = nullptr;
     cudaEvent_t out_ready = nullptr, out_done = nullptr;
     double* out_dev = nullptr;              // pre, uc, vc, wc on the device
-    double* out_host = nullptr;             // pinned copy
+    double* out_host = nullptr;             // pinned staging for pageable destinations
+    double* out_dst[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool out_staged[4] = {false, false, false, false};
+    size_t out_n = 0;
     bool out_pending = false;
 };
 
@@ -171,6 +174,28 @@ int dalloc(ntcfd_ctx* ctx, T** ptr, size_t n) {
     ctx->allocs.push_back(q);
     *ptr = reinterpret_cast<T*>(q);
     return 0;
+}
+
+// True when the copy engine reaches p directly: pinned (page-locked or
+// registered) host memory, device or managed memory.  Ordinary pageable
+// memory reports cudaMemoryTypeUnregistered.
+bool dma_reachable(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost || a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Stream host function of ntcfd_output_async: moves the staged fields into
+// the caller's pageable arrays on the driver's callback thread, so the
+// caller's thread keeps issuing steps meanwhile.  It makes no CUDA call.
+void CUDART_CB scatter_output(void* arg) {
+    auto* ctx = static_cast<ntcfd_ctx*>(arg);
+    const size_t n = ctx->out_n;
+    for (int q = 0; q < 4; ++q)
+        if (ctx->out_staged[q]) std::memcpy(ctx->out_dst[q], ctx->out_host + q * n, n * sizeof(double));
 }
 
 dim3 grid3(const Geom& g, dim3 b) {
@@ -1148,24 +1173,31 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     return records_to_info(ctx, rec.data(), nsteps, info, aoa.data());
 }
 
-int ntcfd_output_async(ntcfd_ctx* ctx) {
+int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
     DEV();
     if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "metrics not set");
     const Geom& g = ctx->g;
     const size_t n = (size_t)g.nx * g.ny * g.nz;
+    if (ctx->out_pending) {   // one output in flight: its buffers are reused
+        CK(cudaEventSynchronize(ctx->out_done));
+        ctx->out_pending = false;
+    }
+    double* dst[4] = {pre, uc, vc, wc};
+    bool staged[4] = {false, false, false, false}, any_staged = false;
+    for (int q = 0; q < 4; ++q) {
+        if (!dst[q]) continue;
+        staged[q] = !dma_reachable(dst[q]);
+        any_staged |= staged[q];
+    }
     if (!ctx->out_dev) {
         double* q = nullptr;
         if (int rc = dalloc(ctx, &q, 4 * n)) return rc;
         ctx->out_dev = q;
-        CK(cudaMallocHost(&ctx->out_host, 4 * n * sizeof(double)));
         CK(cudaStreamCreateWithFlags(&ctx->out_stream, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&ctx->out_ready, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&ctx->out_done, cudaEventDisableTiming));
     }
-    if (ctx->out_pending) {   // one copy in flight: the buffers are reused
-        CK(cudaEventSynchronize(ctx->out_done));
-        ctx->out_pending = false;
-    }
+    if (any_staged && !ctx->out_host) CK(cudaMallocHost(&ctx->out_host, 4 * n * sizeof(double)));
     double* o = ctx->out_dev;
     const dim3 b3(32, 4, 2);
     k_centre<<<grid3(g, b3), b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->p, ctx->faceW,
@@ -1174,21 +1206,25 @@ int ntcfd_output_async(ntcfd_ctx* ctx) {
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->out_ready, ctx->stream));
     CK(cudaStreamWaitEvent(ctx->out_stream, ctx->out_ready, 0));
-    CK(cudaMemcpyAsync(ctx->out_host, o, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->out_stream));
+    for (int q = 0; q < 4; ++q) {
+        ctx->out_dst[q] = dst[q];
+        ctx->out_staged[q] = staged[q];
+        if (!dst[q]) continue;
+        double* to = staged[q] ? ctx->out_host + q * n : dst[q];
+        CK(cudaMemcpyAsync(to, o + q * n, n * sizeof(double), cudaMemcpyDefault, ctx->out_stream));
+    }
+    ctx->out_n = n;
+    if (any_staged) CK(cudaLaunchHostFunc(ctx->out_stream, scatter_output, ctx));
     CK(cudaEventRecord(ctx->out_done, ctx->out_stream));
     ctx->out_pending = true;
     return 0;
 }
 
-int ntcfd_output_wait(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
+int ntcfd_output_wait(ntcfd_ctx* ctx) {
     DEV();
     if (!ctx->out_pending) return fail(ctx, NTCFD_ESTATE, "no ntcfd_output_async in flight");
     CK(cudaEventSynchronize(ctx->out_done));
     ctx->out_pending = false;
-    const size_t n = (size_t)ctx->g.nx * ctx->g.ny * ctx->g.nz;
-    double* dst[4] = {pre, uc, vc, wc};
-    for (int q = 0; q < 4; ++q)
-        if (dst[q]) std::memcpy(dst[q], ctx->out_host + q * n, n * sizeof(double));
     return 0;
 }
 

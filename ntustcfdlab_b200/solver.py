@@ -117,6 +117,7 @@ class Solver:
         self.lib = abi.load_library()
         self.prm = params
         self.nx, self.ny, self.nz = params.nx, params.ny, params.nz
+        self._out = None                # arrays of an output_async in flight
         h = ctypes.c_void_p()
         rc = self.lib.ntcfd_create(ctypes.byref(params), ctypes.byref(h))
         self.h = h
@@ -229,15 +230,23 @@ class Solver:
         self._check(self.lib.ntcfd_set_dynamic_aoa(self.h, dptr(az), dptr(ay), len(az), aoa1, reduce_frequency,
                                                    zc, yc, start_step))
 
-    def output_async(self):
-        """Start the centred output of the last step without waiting for it."""
-        self._check(self.lib.ntcfd_output_async(self.h))
+    def output_async(self, out=None):
+        """Start the centred output of the last step without waiting for it.
+        `out`: four (nx,ny,nz) Fortran-order float64 arrays to fill (pinned
+        ones are written by the copy engine directly), else new ones; they
+        are not to be read before output_wait."""
+        if out is None:
+            out = [np.zeros(self.inner_shape, dtype=np.float64, order="F") for _ in range(4)]
+        for a in out:
+            assert a.dtype == np.float64 and a.flags.f_contiguous and a.shape == self.inner_shape
+        self._check(self.lib.ntcfd_output_async(self.h, *[dptr(a) for a in out]))
+        self._out = tuple(out)
 
     def output_wait(self):
         """(pre, uc, vc, wc) of the last output_async."""
-        arrs = [np.zeros(self.inner_shape, dtype=np.float64, order="F") for _ in range(4)]
-        self._check(self.lib.ntcfd_output_wait(self.h, *[dptr(a) for a in arrs]))
-        return tuple(arrs)
+        self._check(self.lib.ntcfd_output_wait(self.h))
+        out, self._out = self._out, None
+        return out
 
     def step(self, nsteps: int = 1):
         """Runs the loop body nsteps times; returns (list of NtcfdStepInfo, status).

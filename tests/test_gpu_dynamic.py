@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 from conftest import interior, rel_l2
-from ntustcfdlab_b200.abi import f4, make_params, params_copy
+from ntustcfdlab_b200.abi import dptr, f4, make_params, params_copy
 
 pytestmark = pytest.mark.gpu
 
@@ -83,26 +83,44 @@ def test_adjoint_refuses_a_moving_mask():
         s.close()
 
 
-def test_async_output_equals_get_output():
+@pytest.mark.parametrize("pinned", [False, True])
+def test_async_output_equals_get_output(pinned):
+    import torch
     from ntustcfdlab_b200 import cases
     from ntustcfdlab_b200.solver import NtcfdError, Solver
     c = cases.cavity(24, 100.0, 1e-3, 10)
     s = Solver(c.params, c.grid)
+
+    def buffers():
+        if not pinned:     # pageable: staged, then scattered by the stream callback
+            return [np.full(s.inner_shape, -1.0, order="F") for _ in range(4)]
+        n = int(np.prod(s.inner_shape))
+        return [torch.full((n,), -1.0, dtype=torch.float64, pin_memory=True).numpy()
+                .reshape(s.inner_shape, order="F") for _ in range(4)]
     try:
         s.boundary_conditions()
         with pytest.raises(NtcfdError):
             s.output_wait()                                  # nothing in flight
         s.step(3)
-        s.output_async()
+        s.output_async(buffers())
         ref = s.get_output()
         s.step(2)                                            # overlaps the copy
         got = s.output_wait()
         for a, b in zip(got, ref):
             assert np.array_equal(a, b)
-        s.output_async()
-        s.output_async()                                     # waits for the first
-        got2 = s.output_wait()
-        for a, b in zip(got2, s.get_output()):
+        ref = s.get_output()
+        first = buffers()
+        s.output_async(first)
+        s.output_async(buffers())                            # waits for the first
+        for a, b in zip(first, ref):
             assert np.array_equal(a, b)
+        got2 = s.output_wait()
+        for a, b in zip(got2, ref):
+            assert np.array_equal(a, b)
+        some = buffers()                                     # NULL fields are skipped
+        assert s.lib.ntcfd_output_async(s.h, dptr(some[0]), None, None, dptr(some[3])) == 0
+        assert s.lib.ntcfd_output_wait(s.h) == 0
+        assert np.array_equal(some[0], ref[0]) and np.array_equal(some[3], ref[3])
+        assert np.all(some[1] == -1.0) and np.all(some[2] == -1.0)
     finally:
         s.close()
