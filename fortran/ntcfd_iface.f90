@@ -19,6 +19,7 @@ module ntcfd_iface
    integer(c_int), parameter :: NTCFD_WEST = 0, NTCFD_EAST = 1, NTCFD_SOUTH = 2, &
                                 NTCFD_NORTH = 3, NTCFD_BACK = 4, NTCFD_FRONT = 5
    integer(c_int), parameter :: NTCFD_FP64 = 0, NTCFD_MIXED = 1
+   integer(c_int), parameter :: NTCFD_QUICK_CENTRE = 0, NTCFD_QUICK = 1, NTCFD_UPWIND = 2, NTCFD_CENTRE = 3
    integer(c_int), parameter :: NTCFD_SMAG_REF_ALIASED = 0, NTCFD_SMAG_STAGGERED = 1
    integer(c_int), parameter :: NTCFD_SOR_AUTO = 0, NTCFD_SOR_STREAMING = 1, NTCFD_SOR_RESIDENT = 2
 

@@ -50,7 +50,13 @@ enum { NTCFD_BC_NOSLIP = 0, NTCFD_BC_NEUMANN = 1, NTCFD_BC_DIRICHLET = 2,
 enum { NTCFD_WEST = 0, NTCFD_EAST = 1, NTCFD_SOUTH = 2, NTCFD_NORTH = 3,
        NTCFD_BACK = 4, NTCFD_FRONT = 5 };
 enum { NTCFD_FP64 = 0, NTCFD_MIXED = 1 };
-enum { NTCFD_QUICK_CENTRE = 0 };                       /* discretisation_QUICK_centre.f90 */
+/* K2 predictor: discretisation_QUICK_centre.f90 (the one main.f90:213 calls),
+ * or the reference's uncalled alternatives discretisation_QUICK.f90,
+ * discretisation_upwind.f90, discretisation_centre.f90, with their flag Q1
+ * read as LES and their own inline eddy viscosity.  The alternatives predict
+ * u* on i < nx, v* on j < ny, w* on k < nz (the wall faces keep u), and
+ * ntcfd_adjoint does not differentiate them. */
+enum { NTCFD_QUICK_CENTRE = 0, NTCFD_QUICK = 1, NTCFD_UPWIND = 2, NTCFD_CENTRE = 3 };
 enum { NTCFD_SMAG_REF_ALIASED = 0, NTCFD_SMAG_STAGGERED = 1 };
 enum { NTCFD_SOR_REDBLACK = 0, NTCFD_SOR_LEX = 1 };    /* LEX: oracle only */
 /* How the sweeps of one correction cycle run on the device:
@@ -71,7 +77,7 @@ typedef struct ntcfd_params {
     int itmax;               /* SOR sweep cap (main.f90:48) */
     int LES;                 /* 1: add Smagorinsky nu_t (main.f90:60) */
     double Cs;               /* Smagorinsky constant (variables_module.f90:277) */
-    int scheme;              /* NTCFD_QUICK_CENTRE */
+    int scheme;              /* NTCFD_QUICK_CENTRE (default), NTCFD_QUICK, NTCFD_UPWIND, NTCFD_CENTRE */
     int precision;           /* NTCFD_FP64 or NTCFD_MIXED */
     int sor_order;           /* NTCFD_SOR_REDBLACK on the device */
     int smag_mode;           /* NTCFD_SMAG_REF_ALIASED (reference indexing) or _STAGGERED */

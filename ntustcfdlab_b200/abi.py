@@ -26,7 +26,7 @@ NTCFD_ETIMEOUT = -6
 BC_NOSLIP, BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC = 0, 1, 2, 3
 WEST, EAST, SOUTH, NORTH, BACK, FRONT = 0, 1, 2, 3, 4, 5
 FP64, MIXED = 0, 1
-QUICK_CENTRE = 0
+QUICK_CENTRE, QUICK, UPWIND, CENTRE = 0, 1, 2, 3   # K2 schemes (discretisation_*.f90)
 SMAG_REF_ALIASED, SMAG_STAGGERED = 0, 1
 SOR_REDBLACK, SOR_LEX = 0, 1
 SOR_AUTO, SOR_STREAMING, SOR_RESIDENT = 0, 1, 2
@@ -110,14 +110,15 @@ def make_params(nx, ny, nz, *, Re, dt, omega=1.5, zeta=f4(1e-4), itmax=3000, LES
                 Cs=f4(0.18), precision=FP64, sor_order=SOR_REDBLACK,
                 smag_mode=SMAG_REF_ALIASED, check_every=1, bc=None, bc_value=None,
                 u_solid=(0.0, 0.0, 0.0), lx=1.0, mixed_cycle=0,
-                diag_divergence=0, device=0, sor_path=SOR_AUTO, eager=0) -> NtcfdParams:
+                diag_divergence=0, device=0, sor_path=SOR_AUTO, eager=0,
+                scheme=QUICK_CENTRE) -> NtcfdParams:
     """Builds an ``ntcfd_params``.  ``bc`` maps wall name -> (u, v, w) kind
     strings; missing walls are no-slip, as in variables_module.f90:110-132."""
     p = NtcfdParams()
     p.nx, p.ny, p.nz = nx, ny, nz
     p.Re, p.dt, p.omega, p.zeta = Re, dt, omega, zeta
     p.itmax, p.LES, p.Cs = itmax, LES, Cs
-    p.scheme, p.precision, p.sor_order = QUICK_CENTRE, precision, sor_order
+    p.scheme, p.precision, p.sor_order = scheme, precision, sor_order
     p.smag_mode, p.check_every = smag_mode, check_every
     bc = bc or {}
     bc_value = bc_value or {}

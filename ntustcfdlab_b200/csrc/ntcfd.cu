@@ -24,6 +24,7 @@
 #include "k_adjoint.cuh"
 #include "k_mask.cuh"
 #include "k_predictor.cuh"
+#include "k_schemes.cuh"
 #include "k_pressure.cuh"
 #include "k_project.cuh"
 #include "k_resident.cuh"
@@ -340,6 +341,25 @@ bool plan_resident(ntcfd_ctx* ctx) {
     return true;
 }
 
+// K1 + K2 of the configured scheme on stream st, outside a graph: the
+// Smagorinsky pass feeds only the QUICK_centre predictor; the other schemes
+// evaluate their eddy viscosity inline.
+void launch_predictor(ntcfd_ctx* ctx, cudaStream_t st) {
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    const bool qc = P.scheme == NTCFD_QUICK_CENTRE;
+    if (P.LES && qc)
+        k_smagorinsky<<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
+                                         P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
+    const PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
+                      P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
+    if (qc) k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
+    else if (P.scheme == NTCFD_QUICK) k_predictor_scheme<kSchemeQuick><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
+    else if (P.scheme == NTCFD_UPWIND) k_predictor_scheme<kSchemeUpwind><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
+    else k_predictor_scheme<kSchemeCentre><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
+}
+
 // The step graph:
 //   [K1 smag] -> K2 predictor -> K3a rhs -> begin -> WHILE(outer){ defect ->
 //   WHILE(inner){ c x (red, black) -> check } -> correct -> outer_check } ->
@@ -354,15 +374,22 @@ int build_graph(ntcfd_ctx* ctx) {
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     std::vector<cudaGraphNode_t> dep;
     cudaGraphNode_t n;
-    if (P.LES) {
+    const bool qc = P.scheme == NTCFD_QUICK_CENTRE;
+    if (P.LES && qc) {
         GK(add_kernel(&n, G, dep, k_smagorinsky, g3, b3, g, (const double*)ctx->u,
                       (const double*)ctx->v, (const double*)ctx->w, ctx->nut, P.Cs,
                       P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0));
         dep = {n};
     }
-    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
+    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
                 P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
-    GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
+    if (qc) GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
+    else if (P.scheme == NTCFD_QUICK)
+        GK(add_kernel(&n, G, dep, k_predictor_scheme<kSchemeQuick>, g3, b3, g, ctx->tpd, pa, P.Cs));
+    else if (P.scheme == NTCFD_UPWIND)
+        GK(add_kernel(&n, G, dep, k_predictor_scheme<kSchemeUpwind>, g3, b3, g, ctx->tpd, pa, P.Cs));
+    else
+        GK(add_kernel(&n, G, dep, k_predictor_scheme<kSchemeCentre>, g3, b3, g, ctx->tpd, pa, P.Cs));
     dep = {n};
     GK(add_kernel(&n, G, dep, k_rhs, g3, b3, g, ctx->scd, (const double*)ctx->u,
                   (const double*)ctx->v, (const double*)ctx->w, (const double*)ctx->us,
@@ -543,12 +570,7 @@ int run_step_eager(ntcfd_ctx* ctx) {
     const ntcfd_params& P = ctx->prm;
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
-    if (P.LES)
-        k_smagorinsky<<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
-                                         P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
-    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
-                P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
-    k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
+    launch_predictor(ctx, st);
     k_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
     Ctl h{};
     if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, P.omega, &h)) return rc;
@@ -586,7 +608,8 @@ int validate(const ntcfd_params* p, std::string* why) {
     if (p->precision != NTCFD_FP64 && p->precision != NTCFD_MIXED) return bad("precision must be NTCFD_FP64 or NTCFD_MIXED");
     if (p->sor_order != NTCFD_SOR_REDBLACK)
         return bad("the device solver is red-black SOR (sor_order = NTCFD_SOR_REDBLACK)");
-    if (p->scheme != NTCFD_QUICK_CENTRE) return bad("scheme must be NTCFD_QUICK_CENTRE");
+    if (p->scheme < NTCFD_QUICK_CENTRE || p->scheme > NTCFD_CENTRE)
+        return bad("scheme must be NTCFD_QUICK_CENTRE, NTCFD_QUICK, NTCFD_UPWIND or NTCFD_CENTRE");
     if (p->sor_path < NTCFD_SOR_AUTO || p->sor_path > NTCFD_SOR_RESIDENT) return bad("bad sor_path");
     if (p->eager != 0 && p->eager != 1) return bad("eager must be 0 or 1");
     if (p->smag_mode != NTCFD_SMAG_REF_ALIASED && p->smag_mode != NTCFD_SMAG_STAGGERED) return bad("bad smag_mode");
@@ -661,14 +684,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
         return 0;
     };
     int rc;
-    PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
-                P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
-    if ((rc = timed([&] {
-             if (P.LES)
-                 k_smagorinsky<<<g3, b3, 0, ctx->stream>>>(g, ctx->u, ctx->v, ctx->w, ctx->nut, P.Cs,
-                                                           P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
-             k_predictor<double><<<g3, b3, 0, ctx->stream>>>(g, ctx->tpd, pa);
-         }, &out->predictor_ms, 1)))
+    if ((rc = timed([&] { launch_predictor(ctx, ctx->stream); }, &out->predictor_ms, 1)))
         return rc;
     if ((rc = timed([&] {
              k_rhs<<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs,
@@ -1851,6 +1867,8 @@ extern "C" int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_a
     if (spec->nsteps < 1) return fail(ctx, NTCFD_EINVAL, "nsteps must be >= 1");
     if (ctx->dyn_start > 0)
         return fail(ctx, NTCFD_EINVAL, "the adjoint holds ETA fixed: switch the dynamic angle of attack off");
+    if (ctx->prm.scheme != NTCFD_QUICK_CENTRE)
+        return fail(ctx, NTCFD_EINVAL, "the adjoint differentiates the NTCFD_QUICK_CENTRE predictor only");
     if (spec->checkpoint_every < 1) return fail(ctx, NTCFD_EINVAL, "checkpoint_every must be >= 1");
     if (!(spec->adj_zeta >= 0.0) || spec->adj_itmax < 0) return fail(ctx, NTCFD_EINVAL, "bad adjoint stop rule");
     if (!(spec->adj_omega >= 0.0 && spec->adj_omega < 2.0))

@@ -482,7 +482,7 @@ void orc_smagorinsky(orc* o) {
 }
 
 // discretisation_QUICK_centre.f90:1-345.
-void orc_predictor(orc* o) {
+static void predictor_quick_centre(orc* o) {
     const int nx = o->nx, ny = o->ny, nz = o->nz;
     F3 &u = o->u, &v = o->v, &w = o->w;
     F1 &iDx = o->iDx, &Dxs = o->Dxs, &iDy = o->iDy, &Dys = o->Dys, &iDz = o->iDz, &Dzs = o->Dzs;
@@ -662,6 +662,276 @@ void orc_predictor(orc* o) {
                                  + nue * dt * ((w(i, j, k + 1) - w(i, j, k)) / iDz(k + 1) - (w(i, j, k) - w(i, j, k - 1)) / iDz(k)) / Dzs(k);
             }
     }
+}
+
+}  // extern "C"
+
+namespace {
+
+// ----------------------------------------------- uncalled K2 schemes ----
+// discretisation_QUICK.f90:1-415, discretisation_upwind.f90:1-275 and
+// discretisation_centre.f90:1-134.  The reference never calls them and
+// cannot compile them (their flag Q1 is undeclared under implicit none);
+// here Q1 is prm.LES.  u* on i = 1..nx-1, v* on j = 1..ny-1, w* on
+// k = 1..nz-1; the wall faces keep the u -> u_star copy of the last
+// boundary_conditions call.  Every expression keeps the reference's operand
+// order; x**0.5 is evaluated as sqrt(x).
+
+// QUICK face value between nodes a and a+1 of the line f(.).  stag: the line
+// runs along the component's own axis (node spacing iD, the factor
+// 0.125 iD(a+1)^2 / Ds), else across it (node spacing Ds, factor
+// 0.125 Ds(a)^2 / iD); pos selects the upstream stencil of the positive
+// branch (discretisation_QUICK.f90:11-33 and their siblings).
+template <class Fn>
+double quick_face_ref(bool pos, bool stag, const Fn& f, int a, F1& iD, F1& Ds) {
+    const double mid = 0.5 * (f(a) + f(a + 1));
+    if (stag) {
+        if (pos)
+            return mid - 0.125 * iD(a + 1) * iD(a + 1) / Ds(a) * ((f(a + 1) - f(a)) / iD(a + 1) - (f(a) - f(a - 1)) / iD(a));
+        return mid - 0.125 * iD(a + 1) * iD(a + 1) / Ds(a + 1) *
+                     ((f(a + 2) - f(a + 1)) / iD(a + 2) - (f(a + 1) - f(a)) / iD(a + 1));
+    }
+    if (pos) return mid - 0.125 * Ds(a) * Ds(a) / iD(a) * ((f(a + 1) - f(a)) / Ds(a) - (f(a) - f(a - 1)) / Ds(a - 1));
+    return mid - 0.125 * Ds(a) * Ds(a) / iD(a + 1) * ((f(a + 2) - f(a + 1)) / Ds(a + 1) - (f(a + 1) - f(a)) / Ds(a));
+}
+
+inline double p2(double x) { return x * x; }
+
+// The Q1 = 1 blocks (discretisation_upwind.f90:66-80, 156-170, 245-259; the
+// same text in the other two files): eddy viscosity at the u, v, w points.
+double nut_u_ref(orc* o, int i, int j, int k) {
+    F3 &u = o->u, &v = o->v, &w = o->w;
+    F1 &Dxs = o->Dxs, &iDy = o->iDy, &iDz = o->iDz;
+    const double Cs = o->prm.Cs;
+    const double delta = std::pow(Dxs(i) * iDy(j) * iDz(k), (double)(1.f / 3.f));
+    const double s =
+        0.5 * (1 / Dxs(i) / Dxs(i)) * p2((u(i + 1, j, k) + u(i, j, k)) - (u(i, j, k) + u(i - 1, j, k))) +
+        0.5 * (1 / iDy(j) / iDy(j)) * p2((v(i + 1, j, k) + v(i, j, k)) - (v(i + 1, j - 1, k) + v(i, j - 1, k))) +
+        0.5 * (1 / iDz(k) / iDz(k)) * p2((w(i + 1, j, k) + w(i, j, k)) - (w(i + 1, j, k - 1) + w(i, j, k - 1))) +
+        p2(0.5 * (1 / iDy(j)) * ((u(i, j + 1, k) + u(i, j, k)) - (u(i, j, k) + u(i, j - 1, k))) +
+           0.5 * (1 / Dxs(i)) * ((v(i + 1, j, k) + v(i + 1, j - 1, k)) - (v(i, j, k) + v(i, j - 1, k)))) +
+        p2(0.5 * (1 / iDz(k)) * ((u(i, j, k + 1) + u(i, j, k)) - (u(i, j, k) + u(i, j, k - 1))) +
+           0.5 * (1 / Dxs(i)) * ((w(i + 1, j, k) + w(i + 1, j, k - 1)) - (w(i, j, k) + w(i, j, k - 1)))) +
+        p2(0.5 * (1 / iDz(k)) * ((v(i + 1, j, k + 1) + v(i, j - 1, k)) - (v(i + 1, j, k - 1) + v(i, j - 1, k))) +
+           0.5 * (1 / iDy(j)) * ((w(i + 1, j + 1, k) + w(i, j, k - 1)) - (w(i + 1, j - 1, k) + w(i, j, k - 1))));
+    return p2(Cs * delta) * std::sqrt(s);
+}
+
+double nut_v_ref(orc* o, int i, int j, int k) {
+    F3 &u = o->u, &v = o->v, &w = o->w;
+    F1 &iDx = o->iDx, &Dys = o->Dys, &iDz = o->iDz;
+    const double Cs = o->prm.Cs;
+    const double delta = std::pow(iDx(i) * Dys(j) * iDz(k), (double)(1.f / 3.f));
+    const double s =
+        0.5 * (1 / iDx(i) / iDx(i)) * p2((u(i, j + 1, k) + u(i, j, k)) - (u(i - 1, j + 1, k) + u(i - 1, j, k))) +
+        0.5 * (1 / Dys(j) / Dys(j)) * p2((v(i, j + 1, k) + v(i, j, k)) - (v(i, j, k) + v(i, j - 1, k))) +
+        0.5 * (1 / iDz(k) / iDz(k)) * p2((w(i, j + 1, k) + w(i, j, k)) - (w(i, j + 1, k - 1) + w(i, j, k - 1))) +
+        p2(0.5 * (1 / Dys(j)) * ((u(i, j + 1, k) + u(i - 1, j + 1, k)) - (u(i, j, k) + u(i - 1, j, k))) +
+           0.5 * (1 / iDx(i)) * ((v(i + 1, j, k) + v(i, j, k)) - (v(i, j, k) + v(i - 1, j, k)))) +
+        p2(0.5 * (1 / iDz(k)) * ((u(i, j + 1, k + 1) + u(i - 1, j, k)) - (u(i, j + 1, k - 1) + u(i - 1, j, k - 1))) +
+           0.5 * (1 / iDx(i)) * ((w(i + 1, j + 1, k) + w(i, j, k - 1)) - (w(i - 1, j + 1, k) + w(i, j, k - 1)))) +
+        p2(0.5 * (1 / iDz(k)) * ((v(i, j, k + 1) + v(i, j, k)) - (v(i, j, k - 1) + v(i, j, k))) +
+           0.5 * (1 / Dys(j)) * ((w(i, j + 1, k) + w(i, j + 1, k - 1)) - (w(i, j, k) + w(i, j, k - 1))));
+    return p2(Cs * delta) * std::sqrt(s);
+}
+
+double nut_w_ref(orc* o, int i, int j, int k) {
+    F3 &u = o->u, &v = o->v, &w = o->w;
+    F1 &iDx = o->iDx, &iDy = o->iDy, &Dzs = o->Dzs;
+    const double Cs = o->prm.Cs;
+    const double delta = std::pow(iDx(i) * iDy(j) * Dzs(k), (double)(1.f / 3.f));
+    const double s =
+        0.5 * (1 / iDx(i) / iDx(i)) * p2((u(i, j, k + 1) + u(i, j, k)) - (u(i - 1, j, k + 1) + u(i - 1, j, k))) +
+        0.5 * (1 / iDy(j) / iDy(j)) * p2((v(i, j, k + 1) + v(i, j, k)) - (v(i, j - 1, k + 1) + v(i, j - 1, k))) +
+        0.5 * (1 / Dzs(k) / Dzs(k)) * p2((w(i, j, k + 1) + w(i, j, k)) - (w(i, j, k) + w(i, j, k - 1))) +
+        p2(0.5 * (1 / iDy(j)) * ((u(i, j + 1, k) + u(i, j, k)) - (u(i, j, k) + u(i, j - 1, k))) +
+           0.5 * (1 / iDx(i)) * ((v(i + 1, j, k + 1) + v(i, j - 1, k)) - (v(i - 1, j, k + 1) + v(i, j - 1, k)))) +
+        p2(0.5 * (1 / Dzs(k)) * ((u(i, j, k + 1) + u(i - 1, j, k + 1)) - (u(i, j, k) + u(i - 1, j, k))) +
+           0.5 * (1 / iDx(i)) * ((w(i + 1, j, k) + w(i, j, k)) - (w(i - 1, j, k) + w(i, j, k)))) +
+        p2(0.5 * (1 / Dzs(k)) * ((v(i, j, k + 1) + v(i, j - 1, k + 1)) - (v(i, j, k) + v(i, j - 1, k))) +
+           0.5 * (1 / iDy(j)) * ((w(i, j + 1, k) + w(i, j, k)) - (w(i, j - 1, k) + w(i, j, k))));
+    return p2(Cs * delta) * std::sqrt(s);
+}
+
+void predictor_scheme(orc* o) {
+    const int nx = o->nx, ny = o->ny, nz = o->nz, scheme = o->prm.scheme;
+    F3 &u = o->u, &v = o->v, &w = o->w;
+    F1 &iDx = o->iDx, &Dxs = o->Dxs, &iDy = o->iDy, &Dys = o->Dys, &iDz = o->iDz, &Dzs = o->Dzs;
+    const double dt = o->dt, nu = o->nu;
+    const int Q1 = o->prm.LES;
+    const bool quick = scheme == NTCFD_QUICK, upwind = scheme == NTCFD_UPWIND;
+    // upwind face value: the upstream node when the advecting velocity is >= 0
+    auto upw = [](double adv, double up, double down) { return adv >= 0 ? up : down; };
+    // u_star (discretisation_QUICK.f90:7-143, _upwind.f90:7-92, _centre.f90:7-39)
+    for (int k = 1; k <= nz; ++k) {
+#pragma omp parallel for if (par(o)) schedule(static)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx - 1; ++i) {
+                double cx, cy, cz;
+                if (quick) {
+                    const bool pu = u(i, j, k) > 0, pv = v(i, j, k) > 0, pw = w(i, j, k) > 0;
+                    auto ux = [&](int a) { return u(a, j, k); };
+                    auto uy = [&](int a) { return u(i, a, k); };
+                    auto uz = [&](int a) { return u(i, j, a); };
+                    auto vx0 = [&](int a) { return v(a, j, k); };
+                    auto vx1 = [&](int a) { return v(a, j - 1, k); };
+                    auto wx0 = [&](int a) { return w(a, j, k); };
+                    auto wx1 = [&](int a) { return w(a, j, k - 1); };
+                    const double ue = quick_face_ref(pu, true, ux, i, iDx, Dxs);
+                    const double uw = quick_face_ref(pu, true, ux, i - 1, iDx, Dxs);
+                    const double vnu = quick_face_ref(pu, false, vx0, i, iDx, Dxs);
+                    const double vsu = quick_face_ref(pu, false, vx1, i, iDx, Dxs);
+                    const double wfu = quick_face_ref(pu, false, wx0, i, iDx, Dxs);
+                    const double wbu = quick_face_ref(pu, false, wx1, i, iDx, Dxs);
+                    const double un = quick_face_ref(pv, false, uy, j, iDy, Dys);
+                    const double us = quick_face_ref(pv, false, uy, j - 1, iDy, Dys);
+                    const double uf = quick_face_ref(pw, false, uz, k, iDz, Dzs);
+                    const double ub = quick_face_ref(pw, false, uz, k - 1, iDz, Dzs);
+                    cx = dt * (ue * ue - uw * uw) / Dxs(i);
+                    cy = dt * (un * vnu - us * vsu) / iDy(j);
+                    cz = dt * (uf * wfu - ub * wbu) / iDz(k);
+                } else {
+                    const double ut1 = 0.5 * (u(i, j, k) + u(i + 1, j, k));
+                    const double ut2 = upwind ? 0.5 * (u(i - 1, j, k) + u(i, j, k)) : 0.5 * (u(i, j, k) + u(i - 1, j, k));
+                    const double vt1 = 0.5 * (v(i, j, k) + v(i + 1, j, k));
+                    const double vt2 = 0.5 * (v(i, j - 1, k) + v(i + 1, j - 1, k));
+                    const double wt1 = 0.5 * (w(i + 1, j, k) + w(i, j, k));
+                    const double wt2 = 0.5 * (w(i, j, k - 1) + w(i + 1, j, k - 1));
+                    if (upwind) {
+                        cx = dt * (ut1 * upw(ut1, u(i, j, k), u(i + 1, j, k)) - ut2 * upw(ut2, u(i - 1, j, k), u(i, j, k))) / Dxs(i);
+                        cy = dt * (vt1 * upw(vt1, u(i, j, k), u(i, j + 1, k)) - vt2 * upw(vt2, u(i, j - 1, k), u(i, j, k))) / iDy(j);
+                        cz = dt * (wt1 * upw(wt1, u(i, j, k), u(i, j, k + 1)) - wt2 * upw(wt2, u(i, j, k - 1), u(i, j, k))) / iDz(k);
+                    } else {
+                        cx = dt * 0.5 * (ut1 * (u(i, j, k) + u(i + 1, j, k)) - ut2 * (u(i, j, k) + u(i - 1, j, k))) / Dxs(i);
+                        cy = dt * 0.5 * (vt1 * (u(i, j, k) + u(i, j + 1, k)) - vt2 * (u(i, j, k) + u(i, j - 1, k))) / iDy(j);
+                        cz = dt * 0.5 * (wt1 * (u(i, j, k) + u(i, j, k + 1)) - wt2 * (u(i, j, k) + u(i, j, k - 1))) / iDz(k);
+                    }
+                }
+                const double nut = Q1 == 1 ? nut_u_ref(o, i, j, k) : 0.0;
+                const double nue = nu + nut * Q1;
+                o->us(i, j, k) = u(i, j, k) - cx - cy - cz
+                    + nue * dt * ((u(i + 1, j, k) - u(i, j, k)) / iDx(i + 1) - (u(i, j, k) - u(i - 1, j, k)) / iDx(i)) / Dxs(i)
+                    + nue * dt * ((u(i, j + 1, k) - u(i, j, k)) / Dys(j) - (u(i, j, k) - u(i, j - 1, k)) / Dys(j - 1)) / iDy(j)
+                    + nue * dt * ((u(i, j, k + 1) - u(i, j, k)) / Dzs(k) - (u(i, j, k) - u(i, j, k - 1)) / Dzs(k - 1)) / iDz(k);
+            }
+    }
+    // v_star (discretisation_QUICK.f90:145-283, _upwind.f90:94-181, _centre.f90:41-84)
+    for (int k = 1; k <= nz; ++k) {
+#pragma omp parallel for if (par(o)) schedule(static)
+        for (int j = 1; j <= ny - 1; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                double cx, cy, cz;
+                if (quick) {
+                    const bool pu = u(i, j, k) > 0, pv = v(i, j, k) > 0, pw = w(i, j, k) > 0;
+                    auto vx = [&](int a) { return v(a, j, k); };
+                    auto vy = [&](int a) { return v(i, a, k); };
+                    auto vz = [&](int a) { return v(i, j, a); };
+                    auto uy0 = [&](int a) { return u(i, a, k); };
+                    auto uy1 = [&](int a) { return u(i - 1, a, k); };
+                    auto wy0 = [&](int a) { return w(i, a, k); };
+                    auto wy1 = [&](int a) { return w(i, a, k - 1); };
+                    const double ve = quick_face_ref(pu, false, vx, i, iDx, Dxs);
+                    const double vw = quick_face_ref(pu, false, vx, i - 1, iDx, Dxs);
+                    const double uev = quick_face_ref(pv, false, uy0, j, iDy, Dys);
+                    const double uwv = quick_face_ref(pv, false, uy1, j, iDy, Dys);
+                    const double vn = quick_face_ref(pv, true, vy, j, iDy, Dys);
+                    const double vs = quick_face_ref(pv, true, vy, j - 1, iDy, Dys);
+                    const double wfv = quick_face_ref(pv, false, wy0, j, iDy, Dys);
+                    const double wbv = quick_face_ref(pv, false, wy1, j, iDy, Dys);
+                    const double vf = quick_face_ref(pw, false, vz, k, iDz, Dzs);
+                    const double vb = quick_face_ref(pw, false, vz, k - 1, iDz, Dzs);
+                    cx = dt * (uev * ve - uwv * vw) / iDx(i);
+                    cy = dt * (vn * vn - vs * vs) / Dys(j);
+                    cz = dt * (vf * wfv - vb * wbv) / iDz(k);
+                } else {
+                    const double ut1 = 0.5 * (u(i, j, k) + u(i, j + 1, k));
+                    const double ut2 = 0.5 * (u(i - 1, j, k) + u(i - 1, j + 1, k));
+                    const double vt1 = 0.5 * (v(i, j, k) + v(i, j + 1, k));
+                    const double vt2 = 0.5 * (v(i, j - 1, k) + v(i, j, k));
+                    const double wt1 = 0.5 * (w(i, j, k) + w(i, j + 1, k));
+                    const double wt2 = 0.5 * (w(i, j, k - 1) + w(i, j + 1, k - 1));
+                    if (upwind) {
+                        cx = dt * (ut1 * upw(ut1, v(i, j, k), v(i + 1, j, k)) - ut2 * upw(ut2, v(i - 1, j, k), v(i, j, k))) / iDx(i);
+                        cy = dt * (vt1 * upw(vt1, v(i, j, k), v(i, j + 1, k)) - vt2 * upw(vt2, v(i, j - 1, k), v(i, j, k))) / Dys(j);
+                        cz = dt * (wt1 * upw(wt1, v(i, j, k), v(i, j, k + 1)) - wt2 * upw(wt2, v(i, j, k - 1), v(i, j, k))) / iDz(k);
+                    } else {
+                        cx = dt * 0.5 * (ut1 * (v(i, j, k) + v(i + 1, j, k)) - ut2 * (v(i, j, k) + v(i - 1, j, k))) / iDx(i);
+                        cy = dt * 0.5 * (vt1 * (v(i, j, k) + v(i, j + 1, k)) - vt2 * (v(i, j, k) + v(i, j - 1, k))) / Dys(j);
+                        cz = dt * 0.5 * (wt1 * (v(i, j, k) + v(i, j, k + 1)) - wt2 * (v(i, j, k) + v(i, j, k - 1))) / iDz(k);
+                    }
+                }
+                const double nut = Q1 == 1 ? nut_v_ref(o, i, j, k) : 0.0;
+                const double nue = nu + nut * Q1;
+                o->vs(i, j, k) = v(i, j, k) - cx - cy - cz
+                    + nue * dt * ((v(i + 1, j, k) - v(i, j, k)) / Dxs(i) - (v(i, j, k) - v(i - 1, j, k)) / Dxs(i - 1)) / iDx(i)
+                    + nue * dt * ((v(i, j + 1, k) - v(i, j, k)) / iDy(j + 1) - (v(i, j, k) - v(i, j - 1, k)) / iDy(j)) / Dys(j)
+                    + nue * dt * ((v(i, j, k + 1) - v(i, j, k)) / Dzs(k) - (v(i, j, k) - v(i, j, k - 1)) / Dzs(k - 1)) / iDz(k);
+            }
+    }
+    // w_star (discretisation_QUICK.f90:285-413, _upwind.f90:183-273, _centre.f90:86-132)
+    for (int k = 1; k <= nz - 1; ++k) {
+#pragma omp parallel for if (par(o)) schedule(static)
+        for (int j = 1; j <= ny; ++j)
+            for (int i = 1; i <= nx; ++i) {
+                double cx, cy, cz;
+                if (quick) {
+                    const bool pu = u(i, j, k) > 0, pv = v(i, j, k) > 0, pw = w(i, j, k) > 0;
+                    auto wx = [&](int a) { return w(a, j, k); };
+                    auto wy = [&](int a) { return w(i, a, k); };
+                    auto wz = [&](int a) { return w(i, j, a); };
+                    auto uz0 = [&](int a) { return u(i, j, a); };
+                    auto uz1 = [&](int a) { return u(i - 1, j, a); };
+                    auto vz0 = [&](int a) { return v(i, j, a); };
+                    auto vz1 = [&](int a) { return v(i, j - 1, a); };
+                    const double we = quick_face_ref(pu, false, wx, i, iDx, Dxs);
+                    const double ww = quick_face_ref(pu, false, wx, i - 1, iDx, Dxs);
+                    const double wn = quick_face_ref(pv, false, wy, j, iDy, Dys);
+                    const double ws = quick_face_ref(pv, false, wy, j - 1, iDy, Dys);
+                    const double uew = quick_face_ref(pw, false, uz0, k, iDz, Dzs);
+                    const double uww = quick_face_ref(pw, false, uz1, k, iDz, Dzs);
+                    const double vnw = quick_face_ref(pw, false, vz0, k, iDz, Dzs);
+                    const double vsw = quick_face_ref(pw, false, vz1, k, iDz, Dzs);
+                    const double wf = quick_face_ref(pw, true, wz, k, iDz, Dzs);
+                    const double wb = quick_face_ref(pw, true, wz, k - 1, iDz, Dzs);
+                    cx = dt * (uew * we - uww * ww) / iDx(i);
+                    cy = dt * (vnw * wn - vsw * ws) / iDy(j);
+                    cz = dt * (wf * wf - wb * wb) / Dzs(k);
+                } else {
+                    const double ut1 = 0.5 * (u(i, j, k + 1) + u(i, j, k));
+                    const double ut2 = 0.5 * (u(i - 1, j, k + 1) + u(i - 1, j, k));
+                    // discretisation_upwind.f90:195 reads v(i+1,j,k+1); the centre file v(i,j,k+1)
+                    const double vt1 = upwind ? 0.5 * (v(i, j, k) + v(i + 1, j, k + 1)) : 0.5 * (v(i, j, k) + v(i, j, k + 1));
+                    const double vt2 = 0.5 * (v(i, j - 1, k + 1) + v(i, j - 1, k));
+                    const double wt1 = 0.5 * (w(i, j, k + 1) + w(i, j, k));
+                    const double wt2 = 0.5 * (w(i, j, k) + w(i, j, k - 1));
+                    if (upwind) {
+                        cx = dt * (ut1 * upw(ut1, w(i, j, k), w(i + 1, j, k)) - ut2 * upw(ut2, w(i - 1, j, k), w(i, j, k))) / iDx(i);
+                        cy = dt * (vt1 * upw(vt1, w(i, j, k), w(i, j + 1, k)) - vt2 * upw(vt2, w(i, j - 1, k), w(i, j, k))) / iDy(j);
+                        cz = dt * (wt1 * upw(wt1, w(i, j, k), w(i, j, k + 1)) - wt2 * upw(wt2, w(i, j, k - 1), w(i, j, k))) / Dzs(k);
+                    } else {
+                        cx = dt * 0.5 * (ut1 * (w(i, j, k) + w(i + 1, j, k)) - ut2 * (w(i, j, k) + w(i - 1, j, k))) / iDx(i);
+                        cy = dt * 0.5 * (vt1 * (w(i, j, k) + w(i, j + 1, k)) - vt2 * (w(i, j, k) + w(i, j - 1, k))) / iDy(j);
+                        cz = dt * 0.5 * (wt1 * (w(i, j, k) + w(i, j, k + 1)) - wt2 * (w(i, j, k) + w(i, j, k - 1))) / Dzs(k);
+                    }
+                }
+                const double nut = Q1 == 1 ? nut_w_ref(o, i, j, k) : 0.0;
+                const double nue = nu + nut * Q1;
+                o->ws(i, j, k) = w(i, j, k) - cx - cy - cz
+                    + nue * dt * ((w(i + 1, j, k) - w(i, j, k)) / Dxs(i) - (w(i, j, k) - w(i - 1, j, k)) / Dxs(i - 1)) / iDx(i)
+                    + nue * dt * ((w(i, j + 1, k) - w(i, j, k)) / Dys(j) - (w(i, j, k) - w(i, j - 1, k)) / Dys(j - 1)) / iDy(j)
+                    + nue * dt * ((w(i, j, k + 1) - w(i, j, k)) / iDz(k + 1) - (w(i, j, k) - w(i, j, k - 1)) / iDz(k)) / Dzs(k);
+            }
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// K2 of the configured scheme.
+void orc_predictor(orc* o) {
+    if (o->prm.scheme == NTCFD_QUICK_CENTRE) predictor_quick_centre(o);
+    else predictor_scheme(o);
 }
 
 // GS.f90:1-106 -- SOR pressure solve.  LEX follows the reference loop order

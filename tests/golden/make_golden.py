@@ -13,6 +13,9 @@ oracle_*.npz      outputs of the CPU oracle (oracle/, single thread) on small
                   cylinder mask, and the ray-cast mask of the NACA0012.DAT
                   subset.  They freeze the oracle so that a later change to
                   it, or to the device path, shows up as a fixture mismatch.
+oracle_schemes.npz the uncalled predictors discretisation_QUICK.f90,
+                  _upwind.f90 and _centre.f90: per scheme a cavity after 3
+                  steps and two LES steps with a cylinder (interior values).
 """
 from __future__ import annotations
 
@@ -26,8 +29,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from ntustcfdlab_b200.abi import (SOR_LEX, SOR_REDBLACK, SMAG_REF_ALIASED, f4,  # noqa: E402
-                                  make_params)
+from ntustcfdlab_b200.abi import (CENTRE, QUICK, SOR_LEX, SOR_REDBLACK, SMAG_REF_ALIASED,  # noqa: E402
+                                  UPWIND, f4, make_params)
 from oracle import cpu_oracle  # noqa: E402
 
 DECIMATE = 10
@@ -41,9 +44,13 @@ NACA_GRID = dict(n=(4, 48, 64), L=(1.0, 3.0, 4.0),
                  aoa=5.0, zc=1.2, yc=1.5)
 
 
-def cavity_params(sor):
+SCHEMES = ((QUICK, "quick"), (UPWIND, "upwind"), (CENTRE, "centre"))
+SCHEME_LES = dict(n=(6, 12, 16), L=(1.0, 3.0, 4.0), forced=(5, 5), seed=11, cyl=(2.05, 1.55, 0.5))
+
+
+def cavity_params(sor, scheme=0):
     n = CAVITY["n"]
-    return make_params(*n, Re=CAVITY["Re"], dt=CAVITY["dt"], sor_order=sor,
+    return make_params(*n, Re=CAVITY["Re"], dt=CAVITY["dt"], sor_order=sor, scheme=scheme,
                        bc={"North": ("Dirichlet", "no-slip", "no-slip")})
 
 
@@ -56,8 +63,17 @@ def les_params():
                        bc=bc, bc_value={"Back": (0.0, 0.1, 1.0)}, lx=LES["L"][0])
 
 
-def les_state(seed=None):
-    n = LES["n"]
+def scheme_les_params(scheme):
+    c = SCHEME_LES
+    bc = {"West": ("periodic",) * 3, "East": ("periodic",) * 3,
+          "South": ("Neumann",) * 3, "North": ("Neumann",) * 3,
+          "Back": ("Dirichlet", "Dirichlet", "Dirichlet"), "Front": ("Neumann",) * 3}
+    return make_params(*c["n"], Re=LES["Re"], dt=LES["dt"], LES=1, Cs=LES["Cs"], scheme=scheme,
+                       bc=bc, bc_value={"Back": (0.0, 0.1, 1.0)}, lx=c["L"][0])
+
+
+def les_state(seed=None, n=None):
+    n = n or LES["n"]
     shape = (n[0] + 4, n[1] + 4, n[2] + 4)
     rng = np.random.default_rng(LES["seed"] if seed is None else seed)
     u = 0.05 * rng.standard_normal(shape)
@@ -91,6 +107,34 @@ def oracle_les_step():
     return out
 
 
+def inner(a):
+    return np.asfortranarray(a[2:-2, 2:-2, 2:-2])
+
+
+def oracle_schemes():
+    out = {}
+    c = SCHEME_LES
+    for scheme, tag in SCHEMES:
+        o = cpu_oracle.Oracle(cavity_params(SOR_REDBLACK, scheme),
+                              cpu_oracle.gridder_equal(*CAVITY["n"], 1.0, 1.0, 1.0))
+        o.initial_conditions()
+        o.boundary_conditions()
+        info = o.step(CAVITY["steps"])
+        for k in "uvwp":
+            out[f"{tag}_cavity_{k}"] = inner(o.get(k))
+        out[f"{tag}_cavity_sweeps"] = np.array([i.sor_iters for i in info])
+        o = cpu_oracle.Oracle(scheme_les_params(scheme), cpu_oracle.gridder_equal(*c["n"], *c["L"]))
+        o.initial_conditions()
+        o.cylinder(*c["cyl"])
+        for k, a in zip("uvwp", les_state(c["seed"], c["n"])):
+            o.set(k, a)
+        o.boundary_conditions()
+        o.step(len(c["forced"]), forced=list(c["forced"]))
+        for k in "uvwp":
+            out[f"{tag}_les_{k}"] = inner(o.get(k))
+    return out
+
+
 def oracle_naca_mask(az, ay):
     g = NACA_GRID
     p = make_params(*g["n"], Re=100.0, dt=f4(1e-3))
@@ -121,6 +165,7 @@ def main():
         f, sweeps = oracle_cavity(sor)
         np.savez_compressed(os.path.join(HERE, f"oracle_cavity_{tag}.npz"), sweeps=sweeps, **f)
     np.savez_compressed(os.path.join(HERE, "oracle_les_cylinder.npz"), **oracle_les_step())
+    np.savez_compressed(os.path.join(HERE, "oracle_schemes.npz"), **oracle_schemes())
     eta, ties = oracle_naca_mask(np.ascontiguousarray(d12[:, 0]), np.ascontiguousarray(d12[:, 1]))
     np.savez_compressed(os.path.join(HERE, "oracle_naca0012_dat_mask.npz"), ETA=eta, ties=np.array([ties]))
     for fn in sorted(os.listdir(HERE)):

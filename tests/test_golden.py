@@ -78,3 +78,17 @@ def test_oracle_raycasting_of_reference_points_matches_fixture(orc):
     eta, ties = mg.oracle_naca_mask(np.ascontiguousarray(d[:, 0]), np.ascontiguousarray(d[:, 1]))
     assert ties == int(g["ties"][0])
     assert np.array_equal(eta, g["ETA"])
+
+
+def test_oracle_schemes_reproduce_fixture():
+    """The uncalled predictors (discretisation_QUICK/_upwind/_centre.f90)."""
+    from oracle import cpu_oracle
+    mg = _mg()
+    got = mg.oracle_schemes()
+    g = _load("oracle_schemes.npz")
+    assert sorted(got) == sorted(g.files)
+    for k in g.files:
+        assert np.array_equal(got[k], g[k]), k
+    # the schemes differ from one another
+    assert not np.array_equal(g["quick_les_u"], g["centre_les_u"])
+    assert not np.array_equal(g["upwind_les_u"], g["centre_les_u"])
