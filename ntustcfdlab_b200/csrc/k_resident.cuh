@@ -4,17 +4,21 @@
 //
 // The interior rows (j,k) are split into nbj x nbk bricks of at most JB x KB
 // rows; CTA b owns brick (b % nbj, b / nbj) and keeps e of both colours for
-// its rows plus a one-row halo in shared memory (colour-split rows of mx
-// entries, see ntcfd_common.cuh), and the defect d of its rows when it fits.
+// its rows in shared memory (colour-split rows of mx entries, see
+// ntcfd_common.cuh; the tile has a one-row ring that stays 0 and stands for
+// the domain's ghost rows), and the defect d of its rows when it fits.
 // A half-sweep updates the CTA's cells of one colour from shared memory,
-// publishes the updated brick-boundary rows to the global e arrays, waits at
-// a grid barrier and copies the neighbours' boundary rows of that colour
-// into its halo.  The sweep count, the stop rule (GS.f90:11,53), the count
+// the brick-boundary rows first: they read the neighbour bricks' rows
+// straight from the global e arrays (L2), where every CTA publishes its own
+// boundary rows as it updates them; then the CTA arrives at a grid barrier,
+// updates its interior rows from shared memory only and waits.  The sweep
+// count, the stop rule (GS.f90:11,53), the count
 // of correction cycles and the final p += e run inside the kernel, and so do
 // the restarts of the
 // defect correction: when a cycle ends on its length (cycle_len sweeps), the
-// kernel adds e to p, passes a grid barrier, recomputes the FP64 defect of
-// its brick (the arithmetic of k_defect) and sweeps on from e = 0.
+// kernel adds e to p, zeroes e (its published boundary rows included),
+// passes a grid barrier, recomputes the FP64 defect of its brick (the
+// arithmetic of k_defect) and sweeps on from e = 0.
 //
 // The grid barrier spins with a bounded number of polls; a CTA that gives
 // up sets bar->err, and every CTA leaves the sweep loop at the next barrier,
@@ -48,15 +52,14 @@ inline size_t resident_smem(const Brick& b, int nx) {
     const size_t brick = (size_t)b.JB * b.KB * b.mx;
     const size_t arrays = sizeof(Tc) * (2 * tile + 2 * (size_t)(nx + 4) + 2 * (size_t)(b.JB + b.KB) +
                                         (b.cache_d ? 2 * brick : 0) + (b.cache_rd ? 2 * brick : 0));
-    // + row table (int4 offsets and four coefficients per row) and halo table (int2 per row)
+    // + row table (int4 offsets and four coefficients per row)
     const size_t rows = (size_t)b.JB * b.KB;
-    return ((arrays + 15) & ~size_t(15)) + rows * (16 + 4 * sizeof(Tc)) + 8 * (size_t)(2 * (b.JB + b.KB));
+    return ((arrays + 15) & ~size_t(15)) + rows * (16 + 4 * sizeof(Tc));
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
 constexpr int kFill = 4;      // elements in flight per lane when a CTA walks its brick
 constexpr int kDefect = 2;    // cells in flight per lane in the in-kernel defect
-constexpr int kHalo = 8;      // halo elements in flight per thread
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -95,7 +98,11 @@ __device__ __forceinline__ void grid_arrive(GridBar* b, unsigned int nblocks, un
     }
 }
 
-__device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int ticket, int* s_flag) {
+// With src non-null, thread 0 also copies *src (read after the barrier) to *dst
+// before the closing CTA barrier, so every thread sees the same value.
+__device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int ticket, int* s_flag,
+                                          const unsigned long long* src = nullptr,
+                                          unsigned long long* dst = nullptr) {
     if (threadIdx.x == 0) {
         int fail = 0;
         unsigned int polls = 0;
@@ -110,15 +117,18 @@ __device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int ticket, int* 
             }
         }
         *s_flag = fail;
+        if (src) *dst = *(const volatile unsigned long long*)src;
     }
     __syncthreads();
     return *s_flag == 0;
 }
 
-__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int nblocks, int* s_flag) {
+__device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int nblocks, int* s_flag,
+                                          const unsigned long long* src = nullptr,
+                                          unsigned long long* dst = nullptr) {
     unsigned int ticket = 0;
     grid_arrive(b, nblocks, ticket);
-    return grid_wait(b, ticket, s_flag);
+    return grid_wait(b, ticket, s_flag, src, dst);
 }
 
 // Row e of a brick's edge ring (jl or kl on the brick boundary), for e < ne,
@@ -175,13 +185,12 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     Tc* const R1 = R0 + brick;
     Tc* const arrays_end = CR ? R1 + brick : (CD ? D1 + brick : D0);
     // row table: per row of the brick, in sweep order (edge rows first), the shared-memory
-    // tile row, the brick row of d/rd, the global colour-split row and (j+k)&1, and the
-    // row's cN, cS, cF, cB; halo table: per halo row, global source row (-1: domain ghost)
-    // and tile row
+    // tile row, the brick row of d/rd, the global colour-split row, and (j+k)&1 plus
+    // four bits (N, S, F, B) set where that neighbour row lies in another brick; and
+    // the row's cN, cS, cF, cB
     const size_t toff = ((size_t)((unsigned char*)arrays_end - smem_raw) + 15) & ~size_t(15);
     int4* const rowT = reinterpret_cast<int4*>(smem_raw + toff);
     Tc* const rowC = reinterpret_cast<Tc*>(rowT + JB * KB);
-    int2* const haloT = reinterpret_cast<int2*>(rowC + 4 * JB * KB);
     constexpr int NWARP = NT / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tid = threadIdx.x;
@@ -215,20 +224,14 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             int jl, kl;
             brick_row(er, nj, nk, nin, nr - nin, jl, kl);
             const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const int far = (jl == nj && j < g.ny ? 2 : 0) | (jl == 1 && j > 1 ? 4 : 0) |
+                            (kl == nk && k < g.nz ? 8 : 0) | (kl == 1 && k > 1 ? 16 : 0);
             rowT[er] = make_int4((kl * RS + jl) * mx, ((kl - 1) * JB + (jl - 1)) * mx,
-                                 ys * (j + 1) + zs * (k + 1), (j + k) & 1);
+                                 ys * (j + 1) + zs * (k + 1), ((j + k) & 1) | far);
             rowC[4 * er + 0] = sc.cN[j];
             rowC[4 * er + 1] = sc.cS[j];
             rowC[4 * er + 2] = sc.cF[k];
             rowC[4 * er + 3] = sc.cB[k];
-        }
-        for (int h = tid; h < 2 * nk + 2 * nj; h += NT) {
-            int jl, kl;
-            if (h < 2 * nk) { kl = h % nk + 1; jl = (h < nk) ? 0 : nj + 1; }
-            else { const int h2 = h - 2 * nk; jl = h2 % nj + 1; kl = (h2 < nj) ? 0 : nk + 1; }
-            const int j = j0 + jl - 1, k = k0 + kl - 1;
-            const bool in = j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;   // domain ghosts stay 0
-            haloT[h] = make_int2(in ? ys * (j + 1) + zs * (k + 1) : -1, (kl * RS + jl) * mx);
         }
     }
     if (CD || CR) {
@@ -305,19 +308,25 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             Tc* W = c ? S1 : S0;
             const Tc* O = c ? S0 : S1;
             Tc* Ec = c ? eBg : eRg;
+            const Tc* Og = c ? eRg : eBg;   // the other colour, as the neighbour bricks publish it
             const Tc* Dg = c ? dBg : dRg;
             const Tc* Rg = c ? rdBg : rdRg;
             const Tc* Ds = c ? D1 : D0;
             const Tc* Rs = c ? R1 : R0;
             // Two passes over the rows (one warp per row, lanes along the row):
             // first the brick-edge rows, which the neighbours need, then arrive
-            // at the grid barrier, then the interior rows, then wait.
+            // at the grid barrier, then the interior rows, then wait.  An edge
+            // row reads a neighbour row that lies in another brick from the
+            // global array (ld.global.cg: it was written by that brick's CTA
+            // before the last barrier); all its other reads are shared memory.
+#pragma unroll
             for (int pass = 0; pass < 2; ++pass) {
                 const bool edge = pass == 0;
                 const int e0r = edge ? 0 : ne, e1r = edge ? ne : nrows;
                 for (int er = e0r + warp; er < e1r; er += NWARP) {
                     const int4 rt = rowT[er];
-                    const int sr = rt.x, dr = rt.y, gr = rt.z, r = rt.w ^ c;
+                    const int sr = rt.x, dr = rt.y, gr = rt.z, r = (rt.w ^ c) & 1;
+                    const int far = edge ? rt.w : 0;
                     const Tc cN = rowC[4 * er], cS = rowC[4 * er + 1], cF = rowC[4 * er + 2],
                              cB = rowC[4 * er + 3];
                     // two cells per lane (t and t + 32), every load issued before any store
@@ -330,10 +339,16 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                         const int iB = okB ? iB0 : iA;
                         const int sA = sr + mA, sB = sr + mB;
                         const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
-                        const Tc oEA = O[sA + r], oWA = O[sA - 1 + r], oNA = O[sA + mx], oSA = O[sA - mx],
-                                 oFA = O[sA + plane], oBA = O[sA - plane];
-                        const Tc oEB = O[sB + r], oWB = O[sB - 1 + r], oNB = O[sB + mx], oSB = O[sB - mx],
-                                 oFB = O[sB + plane], oBB = O[sB - plane];
+                        const Tc oEA = O[sA + r], oWA = O[sA - 1 + r];
+                        const Tc oEB = O[sB + r], oWB = O[sB - 1 + r];
+                        const Tc oNA = (far & 2) ? __ldcg(Og + gr + ys + mA) : O[sA + mx];
+                        const Tc oNB = (far & 2) ? __ldcg(Og + gr + ys + mB) : O[sB + mx];
+                        const Tc oSA = (far & 4) ? __ldcg(Og + gr - ys + mA) : O[sA - mx];
+                        const Tc oSB = (far & 4) ? __ldcg(Og + gr - ys + mB) : O[sB - mx];
+                        const Tc oFA = (far & 8) ? __ldcg(Og + gr + zs + mA) : O[sA + plane];
+                        const Tc oFB = (far & 8) ? __ldcg(Og + gr + zs + mB) : O[sB + plane];
+                        const Tc oBA = (far & 16) ? __ldcg(Og + gr - zs + mA) : O[sA - plane];
+                        const Tc oBB = (far & 16) ? __ldcg(Og + gr - zs + mB) : O[sB - plane];
                         const Tc rdA = CR ? Rs[dr + mA] : __ldg(Rg + gr + mA);
                         const Tc rdB = CR ? Rs[dr + mB] : __ldg(Rg + gr + mB);
                         // d may be rewritten by a restart of this launch, by this CTA only:
@@ -382,42 +397,14 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 }
                 // black half: a full barrier, so that every CTA's max (interior
                 // rows included) is in the ring before anyone reads it
-                if (!grid_sync(bar, nblocks, &s_flag)) {
+                if (!grid_sync(bar, nblocks, &s_flag, &ring[sg % 3], &s_ring)) {
                     failed = true;
                     break;
                 }
-                if (tid == 0) s_ring = *(volatile unsigned long long*)&ring[sg % 3];
             } else if (!grid_wait(bar, ticket, &s_flag)) {
                 failed = true;
                 break;
             }
-            // neighbours' boundary rows of colour c into the halo, flattened over the CTA
-            // so that each thread has all its L2 reads (ld.global.cg: the rows were
-            // written by other CTAs this half-sweep) in flight at once
-            {
-                const int tot = (2 * nk + 2 * nj) * mx;
-                for (int q0 = 0; q0 < tot; q0 += NT * kHalo) {
-                    Tc v[kHalo];
-                    int dst[kHalo];
-#pragma unroll
-                    for (int u = 0; u < kHalo; ++u) {
-                        const int q = q0 + u * NT + tid;
-                        dst[u] = -1;
-                        if (q < tot) {
-                            const int h = q / mx, m = q - h * mx;
-                            const int2 ht = haloT[h];
-                            if (ht.x >= 0) {
-                                v[u] = __ldcg(Ec + ht.x + m);
-                                dst[u] = ht.y + m;
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < kHalo; ++u)
-                        if (dst[u] >= 0) W[dst[u]] = v[u];
-                }
-            }
-            __syncthreads();
         }
         if (failed) break;
         done_c = s + 1;
@@ -437,6 +424,13 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     add_e_to_p();
     __syncthreads();
     for (int q = tid; q < 2 * tile; q += NT) S0[q] = Tc(0);
+    // the published boundary rows too: the neighbour bricks read them as this brick's e
+    for (int q = tid; q < ne * mx; q += NT) {
+        const int er = q / mx, m = q - er * mx;
+        const int gr = rowT[er].z;
+        eRg[gr + m] = Tc(0);
+        eBg[gr + m] = Tc(0);
+    }
     if (!grid_sync(bar, nblocks, &s_flag)) {
         failed = true;
         break;
