@@ -445,13 +445,18 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             const long long c0 = nat(g, 0, j, k);
             const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
             const long long g0 = spl(g, 0, j, k);
+            // the coefficients are loaded with p, not after it: a second round trip
+            // per chunk would double the pass
+            const double cN = scd.cN[j], cS = scd.cS[j], cF = scd.cF[k], cB = scd.cB[k];
             for (int i0 = 1; i0 <= g.nx; i0 += 32 * kDefect) {
                 double pe[kDefect], pw[kDefect], pn[kDefect], ps[kDefect], pf[kDefect], pb[kDefect],
-                    pc[kDefect], bc[kDefect];
+                    pc[kDefect], bc[kDefect], ce[kDefect], cw[kDefect];
 #pragma unroll
                 for (int u = 0; u < kDefect; ++u) {
                     const int i = min(i0 + lane + 32 * u, g.nx);
                     const long long c = c0 + i;
+                    ce[u] = scd.cE[i];
+                    cw[u] = scd.cW[i];
                     pe[u] = __ldcg(p + c + 1);
                     pw[u] = __ldcg(p + c - 1);
                     pn[u] = __ldcg(p + c + g.px);
@@ -465,9 +470,11 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 for (int u = 0; u < kDefect; ++u) {
                     const int i = i0 + lane + 32 * u;
                     if (i > g.nx) continue;
-                    const double sv = scd.cE[i] * pe[u] + scd.cW[i] * pw[u] + scd.cN[j] * pn[u] +
-                                      scd.cS[j] * ps[u] + scd.cF[k] * pf[u] + scd.cB[k] * pb[u];
-                    const double dval = rdiag_of(scd, i, j, k) * sv - bc[u] - pc[u];
+                    const double sv = ce[u] * pe[u] + cw[u] * pw[u] + cN * pn[u] + cS * ps[u] + cF * pf[u] +
+                                      cB * pb[u];
+                    // rdiag_of's sum in its order
+                    const double rd = rcp_rn(((ce[u] + cw[u]) + (cN + cS)) + (cF + cB));
+                    const double dval = rd * sv - bc[u] - pc[u];
                     const int m = (i + 2) >> 1;
                     const bool red = ((i + j + k) & 1) == 0;
                     if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
