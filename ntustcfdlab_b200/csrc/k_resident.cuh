@@ -448,6 +448,11 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             // the coefficients are loaded with p, not after it: a second round trip
             // per chunk would double the pass
             const double cN = scd.cN[j], cS = scd.cS[j], cF = scd.cF[k], cB = scd.cB[k];
+            // rows of this brick (and the frozen ghosts) through L1: this CTA wrote them
+            // itself (stores do not leave stale L1 lines on the writing SM); rows of the
+            // neighbour bricks, written by other SMs, from L2 only
+            const bool nL1 = jl < nj || j == g.ny, sL1 = jl > 1 || j == 1;
+            const bool fL1 = kl < nk || k == g.nz, bL1 = kl > 1 || k == 1;
             for (int i0 = 1; i0 <= g.nx; i0 += 32 * kDefect) {
                 double pe[kDefect], pw[kDefect], pn[kDefect], ps[kDefect], pf[kDefect], pb[kDefect],
                     pc[kDefect], bc[kDefect], ce[kDefect], cw[kDefect];
@@ -457,13 +462,13 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                     const long long c = c0 + i;
                     ce[u] = scd.cE[i];
                     cw[u] = scd.cW[i];
-                    pe[u] = __ldcg(p + c + 1);
-                    pw[u] = __ldcg(p + c - 1);
-                    pn[u] = __ldcg(p + c + g.px);
-                    ps[u] = __ldcg(p + c - g.px);
-                    pf[u] = __ldcg(p + c + g.pz);
-                    pb[u] = __ldcg(p + c - g.pz);
-                    pc[u] = __ldcg(p + c);
+                    pe[u] = __ldca(p + c + 1);
+                    pw[u] = __ldca(p + c - 1);
+                    pn[u] = nL1 ? __ldca(p + c + g.px) : __ldcg(p + c + g.px);
+                    ps[u] = sL1 ? __ldca(p + c - g.px) : __ldcg(p + c - g.px);
+                    pf[u] = fL1 ? __ldca(p + c + g.pz) : __ldcg(p + c + g.pz);
+                    pb[u] = bL1 ? __ldca(p + c - g.pz) : __ldcg(p + c - g.pz);
+                    pc[u] = __ldca(p + c);
                     bc[u] = __ldg(b + c);
                 }
 #pragma unroll
