@@ -102,6 +102,8 @@ struct ntcfd_ctx {
     Ctl* ctl = nullptr;
     StepRec* rec = nullptr;
     int rec_cap = 0;
+    StepRec* rec_host = nullptr;            // pinned copy of the records of one ntcfd_step call
+    int rec_host_cap = 0;
     unsigned long long* slots = nullptr;   // per-sweep max |change| bits
     unsigned long long* divslot = nullptr;
     GridBar* bar = nullptr;                 // grid barrier of the resident SOR kernel
@@ -878,6 +880,7 @@ void ntcfd_destroy(ntcfd_ctx* ctx) {
     if (ctx->graph) cudaGraphDestroy(ctx->graph);
     for (void* q : ctx->allocs) cudaFree(q);
     if (ctx->rec) cudaFree(ctx->rec);
+    if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
     if (ctx->adj_buf) cudaFree(ctx->adj_buf);
     if (ctx->out_stream) cudaStreamSynchronize(ctx->out_stream);
     if (ctx->out_host) cudaFreeHost(ctx->out_host);
@@ -1181,12 +1184,20 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
         t = t + ctx->prm.dt;
     }
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    std::vector<StepRec> rec(nsteps);
-    CK(cudaMemcpyAsync(rec.data(), ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
+    // the records come back into pinned memory: a pageable destination would take the
+    // driver's staged, synchronous copy path on every call
+    if (nsteps > ctx->rec_host_cap) {
+        if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
+        ctx->rec_host = nullptr;
+        ctx->rec_host_cap = 0;
+        CK(cudaMallocHost(&ctx->rec_host, sizeof(StepRec) * std::max(nsteps, 1024)));
+        ctx->rec_host_cap = std::max(nsteps, 1024);
+    }
+    CK(cudaMemcpyAsync(ctx->rec_host, ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
     ctx->istep += nsteps;
-    return records_to_info(ctx, rec.data(), nsteps, info, aoa.data());
+    return records_to_info(ctx, ctx->rec_host, nsteps, info, aoa.data());
 }
 
 int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
