@@ -33,23 +33,46 @@ __device__ __forceinline__ Tc rdiag_of(const SorCoef<Tc>& s, int i, int j, int k
     return rcp_rn(((s.cE[i] + s.cW[i]) + (s.cN[j] + s.cS[j])) + (s.cF[k] + s.cB[k]));
 }
 
+// Column-walking kernel (k_rhs): a 32 x 8 block covers (i, j) and
+// walks the planes of its chunk k0..k1 (chunk = blockIdx.z, chunks of
+// ceil(nz / gridDim.z) planes), carrying the k-1 value in a register, so a
+// cell costs one new load per field along k and the x/y neighbours hit L1.
+constexpr int kWalkBX = 32, kWalkBY = 8, kWalkUnroll = 4;
+
+__device__ __forceinline__ void walk_range(const Geom& g, int& k0, int& k1) {
+    const int kc = (g.nz + (int)gridDim.z - 1) / (int)gridDim.z;
+    k0 = (int)blockIdx.z * kc + 1;
+    k1 = min(g.nz, k0 + kc - 1);
+}
+
 // K3a -- b' on the interior from the predicted velocity (GS.f90:39-41).
 // u*(0,j,k), v*(i,0,k), w*(i,j,0) equal the state's ghosts (the reference
 // copies u into u_star over the whole halo array in boundary_conditions.f90:317-319).
-__global__ void __launch_bounds__(256) k_rhs(Geom g, SorCoef<double> sc, const double* u,
-                                             const double* v, const double* w, const double* us,
-                                             const double* vs, const double* ws, double* b,
-                                             double dt) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.nx || j > g.ny || k > g.nz) return;
-    const long long c = nat(g, i, j, k);
-    const double uw = (i == 1) ? u[c - 1] : us[c - 1];
-    const double vs_ = (j == 1) ? v[c - g.px] : vs[c - g.px];
-    const double wb = (k == 1) ? w[c - g.pz] : ws[c - g.pz];
-    const double divv = (us[c] - uw) * g.riDx[i] + (vs[c] - vs_) * g.riDy[j] + (ws[c] - wb) * g.riDz[k];
-    b[c] = rdiag_of(sc, i, j, k) * divv / dt;
+__global__ void __launch_bounds__(kWalkBX * kWalkBY) k_rhs(Geom g, SorCoef<double> sc, const double* u,
+                                                          const double* v, const double* w, const double* us,
+                                                          const double* vs, const double* ws, double* b,
+                                                          double dt) {
+    const int i = blockIdx.x * kWalkBX + threadIdx.x + 1;
+    const int j = blockIdx.y * kWalkBY + threadIdx.y + 1;
+    if (i > g.nx || j > g.ny) return;
+    int k0, k1;
+    walk_range(g, k0, k1);
+    if (k0 > k1) return;
+    // rdiag_of's sum, in its order, with the i and j parts hoisted
+    const double sew = sc.cE[i] + sc.cW[i], sns = sc.cN[j] + sc.cS[j];
+    const double rx = g.riDx[i], ry = g.riDy[j];
+    const long long cb = nat(g, i, j, k0);
+    double wb = (k0 == 1) ? w[cb - g.pz] : ws[cb - g.pz];
+#pragma unroll kWalkUnroll
+    for (int k = k0; k <= k1; ++k) {
+        const long long c = cb + (long long)(k - k0) * g.pz;
+        const double uw = (i == 1) ? u[c - 1] : us[c - 1];
+        const double vs_ = (j == 1) ? v[c - g.px] : vs[c - g.px];
+        const double wc = ws[c];
+        const double divv = (us[c] - uw) * rx + (vs[c] - vs_) * ry + (wc - wb) * g.riDz[k];
+        b[c] = rcp_rn((sew + sns) + (sc.cF[k] + sc.cB[k])) * divv / dt;
+        wb = wc;
+    }
 }
 
 // Defect d = rdiag*sum c p0_nb - b' - p0 in double, stored per colour in

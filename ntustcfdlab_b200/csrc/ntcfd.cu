@@ -201,6 +201,17 @@ void CUDART_CB scatter_output(void* arg) {
         if (ctx->out_staged[q]) std::memcpy(ctx->out_dst[q], ctx->out_host + q * n, n * sizeof(double));
 }
 
+// Launch shape of the column-walking kernel k_rhs: 32 x 8 threads
+// over (i, j) and enough chunks of k for about two waves of 8 blocks per SM.
+dim3 walk_block() { return dim3(kWalkBX, kWalkBY, 1); }
+dim3 walk_grid(const Geom& g, int sms) {
+    const int bx = (g.nx + kWalkBX - 1) / kWalkBX, by = (g.ny + kWalkBY - 1) / kWalkBY;
+    int chunks = (2 * 8 * std::max(sms, 1) + bx * by - 1) / (bx * by);
+    chunks = std::max(1, std::min(chunks, g.nz));
+    const int kc = (g.nz + chunks - 1) / chunks;
+    return dim3(bx, by, (g.nz + kc - 1) / kc);
+}
+
 dim3 grid3(const Geom& g, dim3 b) {
     return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, (g.nz + b.z - 1) / b.z);
 }
@@ -393,7 +404,7 @@ int build_graph(ntcfd_ctx* ctx) {
     else
         GK(add_kernel(&n, G, dep, k_predictor_scheme<kSchemeCentre>, g3, b3, g, ctx->tpd, pa, P.Cs));
     dep = {n};
-    GK(add_kernel(&n, G, dep, k_rhs, g3, b3, g, ctx->scd, (const double*)ctx->u,
+    GK(add_kernel(&n, G, dep, k_rhs, walk_grid(g, ctx->sm_count), walk_block(), g, ctx->scd, (const double*)ctx->u,
                   (const double*)ctx->v, (const double*)ctx->w, (const double*)ctx->us,
                   (const double*)ctx->vs, (const double*)ctx->ws, ctx->b, P.dt));
     dep = {n};
@@ -573,7 +584,7 @@ int run_step_eager(ntcfd_ctx* ctx) {
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     launch_predictor(ctx, st);
-    k_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
+    k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
     Ctl h{};
     if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, P.omega, &h)) return rc;
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
@@ -689,7 +700,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     if ((rc = timed([&] { launch_predictor(ctx, ctx->stream); }, &out->predictor_ms, 1)))
         return rc;
     if ((rc = timed([&] {
-             k_rhs<<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs,
+             k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, ctx->stream>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs,
                                                ctx->ws, ctx->b, P.dt);
          }, &out->rhs_ms, 1)))
         return rc;
