@@ -43,6 +43,7 @@ struct Brick {
     int mx;          // colour-split row length (compact index m = 0..mx-1)
     int cache_d;     // 1: d of the brick lives in shared memory too
     int cache_rd;    // 1: rd of the brick lives in shared memory too
+    int narrow;      // 1: the NARROW instance (narrow_rows(nx))
 };
 
 // Dynamic shared memory of k_sor_resident for a brick plan.
@@ -58,6 +59,9 @@ inline size_t resident_smem(const Brick& b, int nx) {
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
+// Rows of at most 32 cells of a colour: the kernel's NARROW instance.
+__host__ __device__ inline bool narrow_rows(int nx) { return (nx + 1) / 2 <= 32; }
+
 constexpr int kFill = 4;      // elements in flight per lane when a CTA walks its brick
 constexpr int kDefect = 2;    // cells in flight per lane in the in-kernel defect
 
@@ -151,7 +155,7 @@ __device__ __forceinline__ void brick_row(int e, int nj, int nk, int ni, int ne,
     }
 }
 
-template <class Tc, int NT, bool CD, bool CR>
+template <class Tc, int NT, bool CD, bool CR, bool NARROW>
 __global__ void __launch_bounds__(NT, 1)
 k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const double* __restrict__ b,
                Tc* __restrict__ eRg,
@@ -200,8 +204,9 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     const int nj = max(0, min(g.ny, j0 + JB - 1) - j0 + 1);
     const int nk = max(0, min(g.nz, k0 + KB - 1) - k0 + 1);
     const int half = (g.nx + 1) / 2;
-    // narrow rows (at most 32 cells of a colour): a lane's two cells lie in two rows
-    const bool narrow = half <= 32;
+    // NARROW (the launch's rows have at most 32 cells of a colour, narrow_rows()): a
+    // lane's two cells lie in two rows
+    constexpr bool narrow = NARROW;
     const int rpw = narrow ? 2 : 1, tstep = narrow ? 32 : 64;
     const int ys = g.mxp, zs = (int)g.mz;   // colour-split row and plane pitch
 
@@ -323,78 +328,133 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             // (ld.global.cg: it was written by that brick's CTA before the last
             // barrier); all its other reads are shared memory.  A lane updates two
             // cells with every load issued before any store: t and t + 32 of one
-            // row, or, when a colour row has at most 32 cells, t of two rows (a
-            // warp then takes two rows at a time).
+            // row, or, in the NARROW instance, t of two rows (a warp then takes two
+            // rows at a time).  The wide loop is kept apart so that it carries none
+            // of the narrow loop's per-cell selects.
 #pragma unroll
             for (int pass = 0; pass < 2; ++pass) {
                 const bool edge = pass == 0;
                 const int e0r = edge ? 0 : ne, e1r = edge ? ne : nrows;
-                for (int er = e0r + warp * rpw; er < e1r; er += NWARP * rpw) {
-                    const int erB = narrow && er + 1 < e1r ? er + 1 : er;
-                    const bool rowB = !narrow || er + 1 < e1r;
-                    const int4 rt = rowT[er], rtB = rowT[erB];
-                    const int sr = rt.x, dr = rt.y, gr = rt.z, r = (rt.w ^ c) & 1;
-                    const int srB = rtB.x, drB = rtB.y, grB = rtB.z, rB = (rtB.w ^ c) & 1;
-                    const int far = edge ? rt.w : 0, farB = edge ? rtB.w : 0;
-                    const Tc cN = rowC[4 * er], cS = rowC[4 * er + 1], cF = rowC[4 * er + 2],
-                             cB = rowC[4 * er + 3];
-                    const Tc cNB = rowC[4 * erB], cSB = rowC[4 * erB + 1], cFB = rowC[4 * erB + 2],
-                             cBB = rowC[4 * erB + 3];
-                    for (int t0 = lane; t0 < half; t0 += tstep) {
-                        const int tB = narrow ? t0 : t0 + 32;
-                        const int iA0 = 2 * t0 + 2 - r, iB0 = 2 * tB + 2 - rB;
-                        const bool okA = iA0 <= g.nx;
-                        const bool okB = rowB && tB < half && iB0 <= g.nx;
-                        if (!okA && !okB) break;
-                        // an invalid cell reuses the other cell's (valid) addresses and is not stored
-                        const int mA0 = t0 + 2 - r, mB0 = tB + 2 - rB;
-                        const int mA = okA ? mA0 : mB0, mB = okB ? mB0 : mA0;
-                        const int iA = okA ? iA0 : iB0, iB = okB ? iB0 : iA0;
-                        const int rAc = okA ? r : rB, rBc = okB ? rB : r;
-                        const int srA = okA ? sr : srB, srBc = okB ? srB : sr;
-                        const int drA = okA ? dr : drB, drBc = okB ? drB : dr;
-                        const int grA = okA ? gr : grB, grBc = okB ? grB : gr;
-                        const int farA = okA ? far : farB, farBc = okB ? farB : far;
-                        const Tc cNA = okA ? cN : cNB, cSA = okA ? cS : cSB, cFA = okA ? cF : cFB,
-                                 cBA = okA ? cB : cBB;
-                        const Tc cNb = okB ? cNB : cN, cSb = okB ? cSB : cS, cFb = okB ? cFB : cF,
-                                 cBb = okB ? cBB : cB;
-                        const int sA = srA + mA, sB = srBc + mB;
-                        const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
-                        const Tc oEA = O[sA + rAc], oWA = O[sA - 1 + rAc];
-                        const Tc oEB = O[sB + rBc], oWB = O[sB - 1 + rBc];
-                        const Tc oNA = (farA & 2) ? __ldcg(Og + grA + ys + mA) : O[sA + mx];
-                        const Tc oNB = (farBc & 2) ? __ldcg(Og + grBc + ys + mB) : O[sB + mx];
-                        const Tc oSA = (farA & 4) ? __ldcg(Og + grA - ys + mA) : O[sA - mx];
-                        const Tc oSB = (farBc & 4) ? __ldcg(Og + grBc - ys + mB) : O[sB - mx];
-                        const Tc oFA = (farA & 8) ? __ldcg(Og + grA + zs + mA) : O[sA + plane];
-                        const Tc oFB = (farBc & 8) ? __ldcg(Og + grBc + zs + mB) : O[sB + plane];
-                        const Tc oBA = (farA & 16) ? __ldcg(Og + grA - zs + mA) : O[sA - plane];
-                        const Tc oBB = (farBc & 16) ? __ldcg(Og + grBc - zs + mB) : O[sB - plane];
-                        const Tc rdA = CR ? Rs[drA + mA] : __ldg(Rg + grA + mA);
-                        const Tc rdB = CR ? Rs[drBc + mB] : __ldg(Rg + grBc + mB);
-                        // d may be rewritten by a restart of this launch, by this CTA only:
-                        // a plain (L1-coherent) load, not the read-only path
-                        const Tc dvA = CD ? Ds[drA + mA] : __ldca(Dg + grA + mA);
-                        const Tc dvB = CD ? Ds[drBc + mB] : __ldca(Dg + grBc + mB);
-                        const Tc e0A = W[sA], e0B = W[sB];
-                        const Tc sumA = eA * oEA + wA * oWA + cNA * oNA + cSA * oSA + cFA * oFA + cBA * oBA;
-                        const Tc sumB = eB * oEB + wB * oWB + cNb * oNB + cSb * oSB + cFb * oFB + cBb * oBB;
-                        const Tc diffA = (rdA * sumA + dvA) - e0A;
-                        const Tc diffB = (rdB * sumB + dvB) - e0B;
-                        const Tc e1A = e0A + om * diffA;
-                        const Tc e1B = e0B + om * diffB;
-                        if (okA) {
+                if constexpr (!NARROW) {
+                    for (int er = e0r + warp; er < e1r; er += NWARP) {
+                        const int4 rt = rowT[er];
+                        const int sr = rt.x, dr = rt.y, gr = rt.z, r = (rt.w ^ c) & 1;
+                        const int far = edge ? rt.w : 0;
+                        const Tc cN = rowC[4 * er], cS = rowC[4 * er + 1], cF = rowC[4 * er + 2],
+                                 cB = rowC[4 * er + 3];
+                        // two cells per lane (t and t + 32), every load issued before any store
+                        for (int t0 = lane; t0 < half; t0 += 64) {
+                            const int tB = t0 + 32;
+                            const int iA = 2 * t0 + 2 - r, iB0 = 2 * tB + 2 - r;
+                            if (iA > g.nx) break;
+                            const bool okB = tB < half && iB0 <= g.nx;
+                            const int mA = t0 + 2 - r, mB = okB ? tB + 2 - r : mA;
+                            const int iB = okB ? iB0 : iA;
+                            const int sA = sr + mA, sB = sr + mB;
+                            const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
+                            const Tc oEA = O[sA + r], oWA = O[sA - 1 + r];
+                            const Tc oEB = O[sB + r], oWB = O[sB - 1 + r];
+                            const Tc oNA = (far & 2) ? __ldcg(Og + gr + ys + mA) : O[sA + mx];
+                            const Tc oNB = (far & 2) ? __ldcg(Og + gr + ys + mB) : O[sB + mx];
+                            const Tc oSA = (far & 4) ? __ldcg(Og + gr - ys + mA) : O[sA - mx];
+                            const Tc oSB = (far & 4) ? __ldcg(Og + gr - ys + mB) : O[sB - mx];
+                            const Tc oFA = (far & 8) ? __ldcg(Og + gr + zs + mA) : O[sA + plane];
+                            const Tc oFB = (far & 8) ? __ldcg(Og + gr + zs + mB) : O[sB + plane];
+                            const Tc oBA = (far & 16) ? __ldcg(Og + gr - zs + mA) : O[sA - plane];
+                            const Tc oBB = (far & 16) ? __ldcg(Og + gr - zs + mB) : O[sB - plane];
+                            const Tc rdA = CR ? Rs[dr + mA] : __ldg(Rg + gr + mA);
+                            const Tc rdB = CR ? Rs[dr + mB] : __ldg(Rg + gr + mB);
+                            // d may be rewritten by a restart of this launch, by this CTA only:
+                            // a plain (L1-coherent) load, not the read-only path
+                            const Tc dvA = CD ? Ds[dr + mA] : __ldca(Dg + gr + mA);
+                            const Tc dvB = CD ? Ds[dr + mB] : __ldca(Dg + gr + mB);
+                            const Tc e0A = W[sA], e0B = W[sB];
+                            const Tc sumA = eA * oEA + wA * oWA + cN * oNA + cS * oSA + cF * oFA + cB * oBA;
+                            const Tc sumB = eB * oEB + wB * oWB + cN * oNB + cS * oSB + cF * oFB + cB * oBB;
+                            const Tc diffA = (rdA * sumA + dvA) - e0A;
+                            const Tc diffB = (rdB * sumB + dvB) - e0B;
+                            const Tc e1A = e0A + om * diffA;
+                            const Tc e1B = e0B + om * diffB;
                             W[sA] = e1A;
-                            if (edge) Ec[grA + mA] = e1A;
+                            if (edge) Ec[gr + mA] = e1A;
                             const B dbA = abs_bits(diffA);
                             ch = dbA > ch ? dbA : ch;
+                            if (okB) {
+                                W[sB] = e1B;
+                                if (edge) Ec[gr + mB] = e1B;
+                                const B dbB = abs_bits(diffB);
+                                ch = dbB > ch ? dbB : ch;
+                            }
                         }
-                        if (okB) {
-                            W[sB] = e1B;
-                            if (edge) Ec[grBc + mB] = e1B;
-                            const B dbB = abs_bits(diffB);
-                            ch = dbB > ch ? dbB : ch;
+                    }
+                } else {
+                    for (int er = e0r + warp * rpw; er < e1r; er += NWARP * rpw) {
+                        const int erB = narrow && er + 1 < e1r ? er + 1 : er;
+                        const bool rowB = !narrow || er + 1 < e1r;
+                        const int4 rt = rowT[er], rtB = rowT[erB];
+                        const int sr = rt.x, dr = rt.y, gr = rt.z, r = (rt.w ^ c) & 1;
+                        const int srB = rtB.x, drB = rtB.y, grB = rtB.z, rB = (rtB.w ^ c) & 1;
+                        const int far = edge ? rt.w : 0, farB = edge ? rtB.w : 0;
+                        const Tc cN = rowC[4 * er], cS = rowC[4 * er + 1], cF = rowC[4 * er + 2],
+                                 cB = rowC[4 * er + 3];
+                        const Tc cNB = rowC[4 * erB], cSB = rowC[4 * erB + 1], cFB = rowC[4 * erB + 2],
+                                 cBB = rowC[4 * erB + 3];
+                        for (int t0 = lane; t0 < half; t0 += tstep) {
+                            const int tB = narrow ? t0 : t0 + 32;
+                            const int iA0 = 2 * t0 + 2 - r, iB0 = 2 * tB + 2 - rB;
+                            const bool okA = iA0 <= g.nx;
+                            const bool okB = rowB && tB < half && iB0 <= g.nx;
+                            if (!okA && !okB) break;
+                            // an invalid cell reuses the other cell's (valid) addresses and is not stored
+                            const int mA0 = t0 + 2 - r, mB0 = tB + 2 - rB;
+                            const int mA = okA ? mA0 : mB0, mB = okB ? mB0 : mA0;
+                            const int iA = okA ? iA0 : iB0, iB = okB ? iB0 : iA0;
+                            const int rAc = okA ? r : rB, rBc = okB ? rB : r;
+                            const int srA = okA ? sr : srB, srBc = okB ? srB : sr;
+                            const int drA = okA ? dr : drB, drBc = okB ? drB : dr;
+                            const int grA = okA ? gr : grB, grBc = okB ? grB : gr;
+                            const int farA = okA ? far : farB, farBc = okB ? farB : far;
+                            const Tc cNA = okA ? cN : cNB, cSA = okA ? cS : cSB, cFA = okA ? cF : cFB,
+                                     cBA = okA ? cB : cBB;
+                            const Tc cNb = okB ? cNB : cN, cSb = okB ? cSB : cS, cFb = okB ? cFB : cF,
+                                     cBb = okB ? cBB : cB;
+                            const int sA = srA + mA, sB = srBc + mB;
+                            const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
+                            const Tc oEA = O[sA + rAc], oWA = O[sA - 1 + rAc];
+                            const Tc oEB = O[sB + rBc], oWB = O[sB - 1 + rBc];
+                            const Tc oNA = (farA & 2) ? __ldcg(Og + grA + ys + mA) : O[sA + mx];
+                            const Tc oNB = (farBc & 2) ? __ldcg(Og + grBc + ys + mB) : O[sB + mx];
+                            const Tc oSA = (farA & 4) ? __ldcg(Og + grA - ys + mA) : O[sA - mx];
+                            const Tc oSB = (farBc & 4) ? __ldcg(Og + grBc - ys + mB) : O[sB - mx];
+                            const Tc oFA = (farA & 8) ? __ldcg(Og + grA + zs + mA) : O[sA + plane];
+                            const Tc oFB = (farBc & 8) ? __ldcg(Og + grBc + zs + mB) : O[sB + plane];
+                            const Tc oBA = (farA & 16) ? __ldcg(Og + grA - zs + mA) : O[sA - plane];
+                            const Tc oBB = (farBc & 16) ? __ldcg(Og + grBc - zs + mB) : O[sB - plane];
+                            const Tc rdA = CR ? Rs[drA + mA] : __ldg(Rg + grA + mA);
+                            const Tc rdB = CR ? Rs[drBc + mB] : __ldg(Rg + grBc + mB);
+                            // d may be rewritten by a restart of this launch, by this CTA only:
+                            // a plain (L1-coherent) load, not the read-only path
+                            const Tc dvA = CD ? Ds[drA + mA] : __ldca(Dg + grA + mA);
+                            const Tc dvB = CD ? Ds[drBc + mB] : __ldca(Dg + grBc + mB);
+                            const Tc e0A = W[sA], e0B = W[sB];
+                            const Tc sumA = eA * oEA + wA * oWA + cNA * oNA + cSA * oSA + cFA * oFA + cBA * oBA;
+                            const Tc sumB = eB * oEB + wB * oWB + cNb * oNB + cSb * oSB + cFb * oFB + cBb * oBB;
+                            const Tc diffA = (rdA * sumA + dvA) - e0A;
+                            const Tc diffB = (rdB * sumB + dvB) - e0B;
+                            const Tc e1A = e0A + om * diffA;
+                            const Tc e1B = e0B + om * diffB;
+                            if (okA) {
+                                W[sA] = e1A;
+                                if (edge) Ec[grA + mA] = e1A;
+                                const B dbA = abs_bits(diffA);
+                                ch = dbA > ch ? dbA : ch;
+                            }
+                            if (okB) {
+                                W[sB] = e1B;
+                                if (edge) Ec[grBc + mB] = e1B;
+                                const B dbB = abs_bits(diffB);
+                                ch = dbB > ch ? dbB : ch;
+                            }
                         }
                     }
                 }

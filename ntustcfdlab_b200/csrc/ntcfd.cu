@@ -294,10 +294,16 @@ using ResidentFn = void (*)(Geom, SorCoef<Tc>, Brick, double*, const double*, Tc
                             const Tc*, Ctl*, GridBar*, double, double, int, int, int, unsigned long long*);
 template <class Tc>
 ResidentFn<Tc> resident_kernel(const Brick& b) {
-    if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true>;
-    if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false>;
-    if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true>;
-    return k_sor_resident<Tc, kResNT, false, false>;
+    if (b.narrow) {
+        if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true, true>;
+        if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false, true>;
+        if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true, true>;
+        return k_sor_resident<Tc, kResNT, false, false, true>;
+    }
+    if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true, false>;
+    if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false, false>;
+    if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true, false>;
+    return k_sor_resident<Tc, kResNT, false, false, false>;
 }
 
 // Brick plan of the resident SOR kernel: the split of the (j,k) rows into at
@@ -319,7 +325,7 @@ bool plan_resident(ntcfd_ctx* ctx) {
             const int JB = (g.ny + nbj - 1) / nbj;
             const int nbj_eff = (g.ny + JB - 1) / JB;
             if ((long long)nbj_eff * nbk_eff > ctx->sm_count) continue;
-            Brick b{nbj_eff, nbk_eff, JB, KB, mx, 0, 0};
+            Brick b{nbj_eff, nbk_eff, JB, KB, mx, 0, 0, narrow_rows(g.nx) ? 1 : 0};
             if (resident_smem<Tc>(b, g.nx) > limit) continue;
             // cache d, then rd, when they fit as well
             b.cache_d = 1;
