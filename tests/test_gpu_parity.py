@@ -128,6 +128,51 @@ def test_streaming_and_resident_paths_agree(prec):
         assert rel_l2(interior(x), interior(y)) <= 1e-12, k
 
 
+# The resident kernel has two instances: rows of at most 32 cells per colour
+# (nx <= 64, every case above) and wider rows.  These cases use nx = 72.
+WIDE = (72, 12, 10)
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_wide_rows_forced_steps_match_oracle(orc, prec):
+    """Two loop bodies with a fixed sweep count on a stretched grid with wide
+    rows, the resident path (the mixed path restarts its correction inside
+    the kernel every 4 sweeps)."""
+    g = orc.gridder_unequal(*WIDE, 2.0, 1.3, 1.7, (12.5, 0.65, 0.6, 16, 4, 6, 4, 6, 1.0, 0.1, 0.3, 0.2, 0.5))
+    p = make_params(*WIDE, Re=100.0, dt=f4(1e-3), zeta=0.0, itmax=9, bc=BCS["mixed"],
+                    bc_value={"Back": (0.3, -0.2, 1.0)}, sor_path=SOR_RESIDENT, precision=prec,
+                    mixed_cycle=4)
+    s, o = _pair(orc, p, g, _random_state(tuple(n + 4 for n in WIDE), 13))
+    try:
+        info, rc = s.step(2)
+        assert all(i.sor_path == SOR_RESIDENT and i.sor_iters == 9 for i in info)
+        o.step(2, forced=[9, 9])
+        # FP32 sweeps with FP64 defect correction reach the FP64 iterate only to the
+        # mixed precision's accuracy
+        _compare(s, o, 1e-12 if prec == FP64 else 1e-5)
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_wide_rows_streaming_and_resident_agree(prec):
+    from ntustcfdlab_b200 import cases
+    res = {}
+    for path in (SOR_STREAMING, SOR_RESIDENT):
+        c = cases.cavity(72, 1000.0, 5e-4, 8, precision=prec)
+        s = _solver(params_copy(c.params, sor_path=path, mixed_cycle=8), c.grid)
+        s.boundary_conditions()
+        info, rc = s.step(c.steps)
+        assert rc == 0 and all(i.sor_path == path for i in info)
+        res[path] = (s.get_state(), [i.sor_iters for i in info], [i.dc_cycles for i in info])
+        s.close()
+    a, b = res[SOR_STREAMING], res[SOR_RESIDENT]
+    assert a[1] == b[1] and a[2] == b[2]
+    assert max(b[2]) > 1           # restarts happened inside the kernel
+    for k, x, y in zip(FIELDS, a[0], b[0]):
+        assert rel_l2(interior(x), interior(y)) <= 1e-12, k
+
+
 @pytest.fixture(scope="module")
 def c1_runs(orc):
     """C1: 40^3 cavity, Re=100, dt=1e-3, lid u=1, zeta=1e-4, 200 steps."""
