@@ -245,14 +245,15 @@ def e2e_run(case, K, isto=100):
     return (t1 - t0), h2d, d2h
 
 
-def cpu_baseline_from(s_gpu, case, seconds):
+def cpu_baseline_from(s_gpu, case, seconds, threads=None):
     """Oracle (the CPU restatement of the reference's algorithm, lexicographic
-    SOR with the reference's OpenMP schedule, all host threads) on a bounded
-    sample: consecutive steps from the device state at the end of the timed
-    run, until `seconds` of CPU time have passed."""
+    SOR with the reference's OpenMP schedule, all host threads unless
+    `threads` is given) on a bounded sample: consecutive steps from the device
+    state at the end of the timed run, until `seconds` of CPU time have
+    passed."""
     from oracle import cpu_oracle
     from ntustcfdlab_b200.abi import SOR_LEX, params_copy
-    threads = os.cpu_count() or 1
+    threads = threads or os.cpu_count() or 1
     o = cpu_oracle.Oracle(params_copy(case.params, sor_order=SOR_LEX), case.grid, threads=threads)
     o.initial_conditions()
     for k, a in zip("uvwp", s_gpu.get_state()):
@@ -446,6 +447,10 @@ def run_ours(args):
                "sample": (f"{nst} consecutive steps ({nsw} SOR sweeps, {el:.1f} s) of the same "
                           f"{args.n}^3 case from the device state after step {K}; lexicographic "
                           f"SOR with the reference's OpenMP schedule, {thr} threads")}
+        # the same sample on one host thread (the reference's serial build)
+        v1, _, nst1, nsw1, el1 = cpu_baseline_from(s, mixed, args.cpu_seconds / 2, threads=1)
+        cpu["single_thread"] = {"value": round(v1, 4), "unit": UNIT, "cores": 1,
+                                "sample": f"{nst1} consecutive steps ({nsw1} SOR sweeps, {el1:.1f} s)"}
     adj = None
     if rank == 0 and world == 1 and not args.no_adjoint:
         adj = adjoint_leg(local, fd=not args.no_fd)
