@@ -222,7 +222,15 @@ int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
  * ntcfd_build_mask_polygon_noalloc apply, checked here).  The angle used is
  * reported in ntcfd_step_info.aoa.  A step whose polygon meets an exact
  * vertex/grid tie stops the call with NTCFD_EINVAL (the reference moves the
- * grid instead).  npts = 0 switches the dynamic angle off. */
+ * grid instead); the steps before it have run, and per_step, ntcfd_time and
+ * the step count account for exactly those.  npts = 0 switches the dynamic
+ * angle off.
+ *
+ * The rebuild uses the allocation-free variant's device array, which every
+ * context on a device shares: two contexts with a dynamic angle of attack on
+ * one device whose ntcfd_step calls overlap (two host threads) race on it and
+ * may build each other's masks.  Run such contexts one after the other, or
+ * on different devices. */
 int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
                           double aoa1, double reduce_frequency, double zc, double yc,
                           int start_step);

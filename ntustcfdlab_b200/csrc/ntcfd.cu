@@ -1169,6 +1169,27 @@ int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_i
     return status;
 }
 
+// End of an ntcfd_step call after `ran` steps were launched: the records of
+// those steps come back (into pinned memory: a pageable destination would take
+// the driver's staged, synchronous copy path on every call), the device time
+// of the call, the step count and the simulated time advance by `ran`.
+int finish_steps(ntcfd_ctx* ctx, int ran, ntcfd_step_info* info, const double* aoa) {
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if (ran > ctx->rec_host_cap) {
+        if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
+        ctx->rec_host = nullptr;
+        ctx->rec_host_cap = 0;
+        CK(cudaMallocHost(&ctx->rec_host, sizeof(StepRec) * std::max(ran, 1024)));
+        ctx->rec_host_cap = std::max(ran, 1024);
+    }
+    if (ran > 0)
+        CK(cudaMemcpyAsync(ctx->rec_host, ctx->rec, sizeof(StepRec) * ran, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    ctx->istep += ran;
+    return records_to_info(ctx, ctx->rec_host, ran, info, aoa);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1195,26 +1216,18 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
             const int rc = ntcfd_build_mask_polygon_noalloc(ctx, ctx->dyn_az.data(), ctx->dyn_ay.data(),
                                                             (int)ctx->dyn_az.size(), aoa[s], ctx->dyn_zc,
                                                             ctx->dyn_yc, &ties);
-            if (rc) return rc;
+            if (rc) {
+                // steps 0..s-1 ran: account for them (time, step count, records) before
+                // returning, so that the host's view matches the device state
+                const std::string why = ctx->err;
+                if (int r2 = finish_steps(ctx, s, info, aoa.data())) return r2;
+                return fail(ctx, rc, "step %lld of this call (%d ran): %s", (long long)s + 1, s, why.c_str());
+            }
         }
         if (int rc = launch_step(ctx)) return rc;
         t = t + ctx->prm.dt;
     }
-    CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    // the records come back into pinned memory: a pageable destination would take the
-    // driver's staged, synchronous copy path on every call
-    if (nsteps > ctx->rec_host_cap) {
-        if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
-        ctx->rec_host = nullptr;
-        ctx->rec_host_cap = 0;
-        CK(cudaMallocHost(&ctx->rec_host, sizeof(StepRec) * std::max(nsteps, 1024)));
-        ctx->rec_host_cap = std::max(nsteps, 1024);
-    }
-    CK(cudaMemcpyAsync(ctx->rec_host, ctx->rec, sizeof(StepRec) * nsteps, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
-    ctx->istep += nsteps;
-    return records_to_info(ctx, ctx->rec_host, nsteps, info, aoa.data());
+    return finish_steps(ctx, nsteps, info, aoa.data());
 }
 
 int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {

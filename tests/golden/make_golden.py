@@ -1,6 +1,6 @@
 """Generates the committed fixtures of tests/golden.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <checkout of the reference>
 
 naca_dat.npz      every 10th point (and the closing point) of the reference's
                   airfoil files NACA0012.DAT and NACA0015.DAT, which
@@ -154,7 +154,8 @@ def read_dat(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True,
+                    help="directory of the reference checkout (holds NACA0012.DAT, NACA0015.DAT)")
     args = ap.parse_args()
     cpu_oracle.build()
     d12 = read_dat(os.path.join(args.reference, "NACA0012.DAT"))

@@ -148,8 +148,8 @@ def test_wide_rows_forced_steps_match_oracle(orc, prec):
         assert all(i.sor_path == SOR_RESIDENT and i.sor_iters == 9 for i in info)
         o.step(2, forced=[9, 9])
         # FP32 sweeps with FP64 defect correction reach the FP64 iterate only to the
-        # mixed precision's accuracy
-        _compare(s, o, 1e-12 if prec == FP64 else 1e-5)
+        # mixed precision's accuracy: the 1e-6 relative L2 target
+        _compare(s, o, 1e-12 if prec == FP64 else 1e-6)
     finally:
         s.close()
 
@@ -240,7 +240,28 @@ def test_mixed_precision_matches_fp64():
     errs = {k: rel_l2(interior(a), interior(b)) for k, a, b in zip(FIELDS, res[1][0], res[0][0])}
     print("mixed vs FP64 rel-L2:", errs, "sweeps", sum(res[0][1]), sum(res[1][1]))
     for k in FIELDS:
-        assert errs[k] < 1e-5, (k, errs[k])
+        assert errs[k] <= 1e-6, (k, errs[k])
+
+
+def test_c2_mixed_within_1e6_of_fp64():
+    """C2 as configured: 128^3 cavity, Re = 1000, dt = 5e-4, 500 steps from
+    rest at zeta = 1e-4.  The mixed path (FP32 sweeps, FP64 defect
+    correction every 8 sweeps) stays within 1e-6 relative L2 of the plain
+    FP64 path in each of u, v, w and p, and both converge every step."""
+    from ntustcfdlab_b200 import cases
+    res = []
+    for prec in (FP64, MIXED):
+        c = cases.c2(precision=prec)
+        s = _solver(params_copy(c.params, mixed_cycle=8 if prec == MIXED else 0), c.grid)
+        s.boundary_conditions()
+        info, rc = s.step(c.steps)
+        assert rc == 0 and all(i.converged for i in info)
+        res.append(s.get_state())
+        s.close()
+    errs = {k: rel_l2(interior(a), interior(b)) for k, a, b in zip(FIELDS, res[1], res[0])}
+    print("C2 mixed vs FP64 rel-L2 after 500 steps:", errs)
+    for k in FIELDS:
+        assert errs[k] <= 1e-6, (k, errs[k])
 
 
 def test_cylinder_mask_exact(orc):

@@ -58,3 +58,24 @@ def test_two_gloo_ranks_reduce_max_and_sum():
     for _, _, _, mx, sm, ref in res:
         assert mx == 15.0 and sm == 2.0
     assert res[1][5] is None
+
+
+@pytest.mark.timeout(120)
+def test_reference_arm_never_loads_the_cuda_library():
+    """bench.py --impl reference times the CPU restatement only: the grid and
+    the parameters are made without libntcfd.so, so the process never maps it."""
+    import json
+    import subprocess
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--n', '12', "
+            "'--steps', '2', '--warmup', '1']; sys.path.insert(0, %r); "
+            "runpy.run_path(%r, run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('MAPPED', 'libntcfd.so' in maps, 'libntcfd_oracle.so' in maps)"
+            % (ROOT, os.path.join(ROOT, "bench.py")))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=110)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["steps"] == 2
+    assert line["sweep_rate"]["unit"] == "Mcell-sweeps/s"
+    assert lines[-1] == "MAPPED False True"

@@ -30,9 +30,9 @@ def _solver_and_polygon():
     return s, np.ascontiguousarray(z), np.ascontiguousarray(y)
 
 
-def _noalloc(s, z, y, aoa):
+def _noalloc(s, z, y, aoa, zc=4.0, yc=4.0):
     ties = ctypes.c_int(-1)
-    rc = s.lib.ntcfd_build_mask_polygon_noalloc(s.h, dptr(z), dptr(y), len(z), aoa, 4.0, 4.0,
+    rc = s.lib.ntcfd_build_mask_polygon_noalloc(s.h, dptr(z), dptr(y), len(z), aoa, zc, yc,
                                                  ctypes.byref(ties))
     return rc, ties.value
 
@@ -61,3 +61,53 @@ def test_noalloc_rejects_inputs_beyond_its_limits():
     assert rc == abi.NTCFD_EINVAL
     assert "at most 16384" in s._err()
     s.close()
+
+
+def test_noalloc_rejects_a_plane_beyond_its_cell_limit():
+    """ny * nz = 513 * 512 > 262144: refused before any device work, with the
+    limit in the message; the context stays usable."""
+    from ntustcfdlab_b200.solver import Solver, gridder_equal
+    n = (3, 513, 512)
+    s = Solver(make_params(*n, Re=100.0, dt=1e-3), gridder_equal(*n, 1.0, 4.0, 4.0))
+    try:
+        z = np.ascontiguousarray([0.5, 1.0, 1.5, 1.0, 0.5])
+        y = np.ascontiguousarray([0.0, 0.31, 0.0, -0.29, 0.0])
+        rc, _ = _noalloc(s, z, y, 3.0, 1.0, 2.0)
+        assert rc == abi.NTCFD_EINVAL
+        assert "at most 262144" in s._err()
+        assert s.build_mask_polygon(z, y, 3.0, 1.0, 2.0) == 0   # the allocating path takes it
+    finally:
+        s.close()
+
+
+def test_noalloc_reports_the_same_ties_as_the_allocating_path():
+    """A diamond whose vertices sit on grid nodes: both entry points count the
+    same exact vertex/grid ties (the reference would move the grid) and
+    refuse the mask; calls after it still work."""
+    from ntustcfdlab_b200.solver import Solver, gridder_equal
+    n = (3, 32, 32)
+    s = Solver(make_params(*n, Re=100.0, dt=1e-3), gridder_equal(*n, 1.0, 4.0, 4.0))
+    try:
+        z = np.ascontiguousarray([0.5, 1.0, 1.5, 1.0, 0.5])
+        y = np.ascontiguousarray([0.0, 0.5, 0.0, -0.5, 0.0])
+        ties_ref = ctypes.c_int(-1)
+        rc_ref = s.lib.ntcfd_build_mask_polygon(s.h, dptr(z), dptr(y), len(z), 0.0, 1.0, 2.0,
+                                                ctypes.byref(ties_ref))
+        assert rc_ref == abi.NTCFD_EINVAL and ties_ref.value > 0
+        for _ in range(2):
+            rc, t = _noalloc(s, z, y, 0.0, 1.0, 2.0)
+            assert rc == abi.NTCFD_EINVAL and t == ties_ref.value
+            assert "ties" in s._err()
+        # a polygon off the nodes (no tie in the oracle either) goes through again:
+        # each call clears the shared tie counter
+        zo, yo = np.ascontiguousarray(z + 0.0123), np.ascontiguousarray(y + 0.0171)
+        rc, t = _noalloc(s, zo, yo, 0.0, 1.0, 2.0)
+        assert rc == 0 and t == 0, s._err()
+        ref = ctypes.c_int(-1)
+        assert s.lib.ntcfd_build_mask_polygon(s.h, dptr(zo), dptr(yo), len(zo), 0.0, 1.0, 2.0,
+                                              ctypes.byref(ref)) == 0
+        eta = s.get_mask()
+        assert _noalloc(s, zo, yo, 0.0, 1.0, 2.0) == (0, 0)
+        np.testing.assert_array_equal(s.get_mask(), eta)
+    finally:
+        s.close()
