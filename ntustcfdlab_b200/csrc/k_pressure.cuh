@@ -33,6 +33,48 @@ __device__ __forceinline__ Tc rdiag_of(const SorCoef<Tc>& s, int i, int j, int k
     return rcp_rn(((s.cE[i] + s.cW[i]) + (s.cN[j] + s.cS[j])) + (s.cF[k] + s.cB[k]));
 }
 
+// Explicitly rounded operations: every kernel that evaluates a sweep or a
+// defect uses these, so the resident and streaming paths round alike
+// whatever the compiler would contract.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
+// One SOR update of a cell of the correction e (GS.f90:43-53 in the form
+// eNew = rdiag * sum_nb c_nb e_nb + d): returns eNew - e0 and the relaxed
+// value e0 + omega (eNew - e0) in *e1.
+template <class Tc>
+__device__ __forceinline__ Tc sor_update(Tc cE, Tc oE, Tc cW, Tc oW, Tc cN, Tc oN, Tc cS, Tc oS, Tc cF,
+                                         Tc oF, Tc cB, Tc oB, Tc rd, Tc d, Tc e0, Tc om, Tc* e1) {
+    Tc s = mul_rn(cE, oE);
+    s = fma_rn(cW, oW, s);
+    s = fma_rn(cN, oN, s);
+    s = fma_rn(cS, oS, s);
+    s = fma_rn(cF, oF, s);
+    s = fma_rn(cB, oB, s);
+    const Tc diff = sub_rn(fma_rn(rd, s, d), e0);
+    *e1 = fma_rn(om, diff, e0);
+    return diff;
+}
+
+// FP64 defect of a cell, d = rdiag * sum_nb c_nb p_nb - b' - p (the reference
+// sweep's fixed-point residual): the same sums as sor_update and rdiag_of.
+__device__ __forceinline__ double defect_value(double cE, double pe, double cW, double pw, double cN, double pn,
+                                               double cS, double ps, double cF, double pf, double cB, double pb,
+                                               double bv, double pc) {
+    double s = mul_rn(cE, pe);
+    s = fma_rn(cW, pw, s);
+    s = fma_rn(cN, pn, s);
+    s = fma_rn(cS, ps, s);
+    s = fma_rn(cF, pf, s);
+    s = fma_rn(cB, pb, s);
+    const double rd = rcp_rn(((cE + cW) + (cN + cS)) + (cF + cB));
+    return sub_rn(fma_rn(rd, s, -bv), pc);
+}
+
 // Column-walking kernel (k_rhs): a 32 x 8 block covers (i, j) and
 // walks the planes of its chunk k0..k1 (chunk = blockIdx.z, chunks of
 // ceil(nz / gridDim.z) planes), carrying the k-1 value in a register, so a
@@ -109,9 +151,8 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
     }
     if (i > g.nx || j > g.ny || k > g.nz) return;
     const long long c = nat(g, i, j, k);
-    const double s = sc.cE[i] * p[c + 1] + sc.cW[i] * p[c - 1] + sc.cN[j] * p[c + g.px] +
-                     sc.cS[j] * p[c - g.px] + sc.cF[k] * p[c + g.pz] + sc.cB[k] * p[c - g.pz];
-    const double d = rdiag_of(sc, i, j, k) * s - b[c] - p[c];
+    const double d = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], sc.cN[j], p[c + g.px], sc.cS[j],
+                                  p[c - g.px], sc.cF[k], p[c + g.pz], sc.cB[k], p[c - g.pz], b[c], p[c]);
     const long long q = spl(g, (i + 2) >> 1, j, k);
     if (((i + j + k) & 1) == 0) { dR[q] = (Tc)d; eR[q] = Tc(0); }
     else { dB[q] = (Tc)d; eB[q] = Tc(0); }
@@ -189,10 +230,10 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
         if (!ok[kk]) continue;
         const int k = k0 + kk;
         const int i = 2 * t + 2 - (((j + k) ^ colour) & 1);
-        const Tc s = sc.cE[i] * nE[kk] + sc.cW[i] * nW[kk] + cN * nN[kk] + cS * nS[kk] +
-                     sc.cF[k] * nF[kk] + sc.cB[k] * nB[kk];
-        const Tc diff = (rd[kk] * s + dd[kk]) - e0[kk];
-        eOwn[q[kk]] = e0[kk] + om * diff;
+        Tc e1;
+        const Tc diff = sor_update(sc.cE[i], nE[kk], sc.cW[i], nW[kk], cN, nN[kk], cS, nS[kk], sc.cF[k], nF[kk],
+                                   sc.cB[k], nB[kk], rd[kk], dd[kk], e0[kk], om, &e1);
+        eOwn[q[kk]] = e1;
         const B db = abs_bits(diff);
         ch = db > ch ? db : ch;
     }
@@ -254,15 +295,14 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
             const Tc nEB = oC[mB + r], nWB = oC[mB - 1 + r], nNB = oN[mB], nSB = oS[mB], nFB = oF[mB],
                      nBB = oB[mB];
             const Tc dA = dR[mA], dB_ = dR[mB], e0A = eR[mA], e0B = eR[mB], rdA = rR[mA], rdB = rR[mB];
-            const Tc sA = eA * nEA + wA * nWA + cN * nNA + cS * nSA + cF * nFA + cB * nBA;
-            const Tc sB = eB * nEB + wB * nWB + cN * nNB + cS * nSB + cF * nFB + cB * nBB;
-            const Tc diffA = (rdA * sA + dA) - e0A;
-            const Tc diffB = (rdB * sB + dB_) - e0B;
-            eR[mA] = e0A + om * diffA;
+            Tc e1A, e1B;
+            const Tc diffA = sor_update(eA, nEA, wA, nWA, cN, nNA, cS, nSA, cF, nFA, cB, nBA, rdA, dA, e0A, om, &e1A);
+            const Tc diffB = sor_update(eB, nEB, wB, nWB, cN, nNB, cS, nSB, cF, nFB, cB, nBB, rdB, dB_, e0B, om, &e1B);
+            eR[mA] = e1A;
             const B dbA = abs_bits(diffA);
             ch = dbA > ch ? dbA : ch;
             if (okB) {
-                eR[mB] = e0B + om * diffB;
+                eR[mB] = e1B;
                 const B dbB = abs_bits(diffB);
                 ch = dbB > ch ? dbB : ch;
             }

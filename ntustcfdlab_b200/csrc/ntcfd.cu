@@ -288,22 +288,22 @@ SorCoef<double> sor_coef<double>(ntcfd_ctx* ctx) { return ctx->scd; }
 template <>
 SorCoef<float> sor_coef<float>(ntcfd_ctx* ctx) { return ctx->scf; }
 
-// The resident SOR kernel for a brick plan (d and rd cached or not).
+// The resident SOR kernel for a brick plan (d and rd cached or not, row shape).
 template <class Tc>
 using ResidentFn = void (*)(Geom, SorCoef<Tc>, Brick, double*, const double*, Tc*, Tc*, Tc*, Tc*, const Tc*,
                             const Tc*, Ctl*, GridBar*, double, double, int, int, int, unsigned long long*);
+template <class Tc, int MODE>
+ResidentFn<Tc> resident_kernel_m(const Brick& b) {
+    if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true, MODE>;
+    if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false, MODE>;
+    if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true, MODE>;
+    return k_sor_resident<Tc, kResNT, false, false, MODE>;
+}
 template <class Tc>
 ResidentFn<Tc> resident_kernel(const Brick& b) {
-    if (b.narrow) {
-        if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true, true>;
-        if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false, true>;
-        if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true, true>;
-        return k_sor_resident<Tc, kResNT, false, false, true>;
-    }
-    if (b.cache_d && b.cache_rd) return k_sor_resident<Tc, kResNT, true, true, false>;
-    if (b.cache_d) return k_sor_resident<Tc, kResNT, true, false, false>;
-    if (b.cache_rd) return k_sor_resident<Tc, kResNT, false, true, false>;
-    return k_sor_resident<Tc, kResNT, false, false, false>;
+    if (b.mode == kResNarrow) return resident_kernel_m<Tc, kResNarrow>(b);
+    if (b.mode == kResWide1) return resident_kernel_m<Tc, kResWide1>(b);
+    return resident_kernel_m<Tc, kResWide>(b);
 }
 
 // Brick plan of the resident SOR kernel: the split of the (j,k) rows into at
@@ -325,7 +325,7 @@ bool plan_resident(ntcfd_ctx* ctx) {
             const int JB = (g.ny + nbj - 1) / nbj;
             const int nbj_eff = (g.ny + JB - 1) / JB;
             if ((long long)nbj_eff * nbk_eff > ctx->sm_count) continue;
-            Brick b{nbj_eff, nbk_eff, JB, KB, mx, 0, 0, narrow_rows(g.nx) ? 1 : 0};
+            Brick b{nbj_eff, nbk_eff, JB, KB, mx, 0, 0, res_mode(g.nx)};
             if (resident_smem<Tc>(b, g.nx) > limit) continue;
             // cache d, then rd, when they fit as well
             b.cache_d = 1;
@@ -421,12 +421,10 @@ int build_graph(ntcfd_ctx* ctx) {
             return fail(ctx, NTCFD_EINVAL, "the resident SOR kernel does not fit this grid on this device");
     }
     if (ctx->resident) {
-        // the resident kernel runs the whole solve (every correction cycle), so the
-        // solve is two plain nodes: the defect (which also starts the solve) and the kernel
+        // the resident kernel runs the whole solve (every defect pass and correction
+        // cycle), so the solve is two plain nodes: the counter reset and the kernel
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
-        GK(add_kernel(&n, G, dep, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
-                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, (cudaGraphConditionalHandle)0, 0,
-                      ctx->ring, (unsigned int*)ctx->bar, 1));
+        GK(add_kernel(&n, G, dep, k_resident_begin, dim3(1), dim3(1), ctx->ctl, ctx->ring, ctx->bar));
         dep = {n};
         GK(add_kernel_ex(&n, G, dep, resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid), dim3(kResNT),
                          ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, (const double*)ctx->b,
@@ -535,9 +533,8 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         return 0;
     };
     if (ctx->resident) {
-        // one defect (starting the solve) and one launch that runs every cycle
-        k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, ctx->ring,
-                                        (unsigned int*)ctx->bar, 1);
+        // the counter reset and one launch that runs every defect pass and cycle
+        k_resident_begin<<<1, 1, 0, st>>>(ctx->ctl, ctx->ring, ctx->bar);
         void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&b, (void*)&eR,
                         (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
                         (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
@@ -726,29 +723,27 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
                  g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
          }, &out->sweep_ms, 2)))
         return rc;
-    // the resident kernel: one launch of `nsw` sweeps (zeta = 0) on a scratch copy of p
+    // the resident kernel: one launch of `nsw` sweeps (zeta = 0, one cycle) on a scratch
+    // copy of p, less a launch of no sweep (the kernel's set-up, first defect and p += e)
     if (ctx->resident) {
         const int nsw = 50;
         double* pscratch = ctx->us;   // rewritten by the predictor every step
         CK(cudaMemcpyAsync(pscratch, ctx->p, ctx->nat_elems * sizeof(double), cudaMemcpyDeviceToDevice,
                            ctx->stream));
-        if ((rc = timed([&] {
-                 k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, pscratch, ctx->b, dR, dB, eR, eB,
-                                                          ctx->ctl, 0, 0, ctx->ring, (unsigned int*)ctx->bar, 0);
-                 int zero = 0;
-                 (void)zero;
-                 cudaMemsetAsync(&ctx->ctl->ik, 0, sizeof(int), ctx->stream);
-                 void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&ctx->b,
-                                 (void*)&eR,
-                                 (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
-                                 (void*)&ctx->ctl, (void*)&ctx->bar,
-                                 (void*)&P.omega, (void*)&kZeroZeta, (void*)&nsw, (void*)&nsw,
-                                 (void*)&kOne, (void*)&ctx->ring};
-                 cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
-                                             dim3(kResNT), args, ctx->res_smem, ctx->stream);
-             }, &out->resident_ms, 1)))
-            return rc;
-        out->resident_ms -= out->defect_ms;
+        auto resident = [&](const int* sweeps) {
+            k_resident_begin<<<1, 1, 0, ctx->stream>>>(ctx->ctl, ctx->ring, ctx->bar);
+            void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&ctx->b,
+                            (void*)&eR, (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
+                            (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&kZeroZeta,
+                            (void*)sweeps, (void*)sweeps, (void*)&kOne, (void*)&ctx->ring};
+            cudaLaunchCooperativeKernel((const void*)resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid),
+                                        dim3(kResNT), args, ctx->res_smem, ctx->stream);
+        };
+        const int none = 0;
+        float t0 = 0.0f;
+        if ((rc = timed([&] { resident(&none); }, &t0, 1))) return rc;
+        if ((rc = timed([&] { resident(&nsw); }, &out->resident_ms, 1))) return rc;
+        out->resident_ms -= t0;
         out->resident_sweeps = (float)nsw;
     }
     // K4 on the predicted velocity in place (us/vs/ws are rewritten every step)
