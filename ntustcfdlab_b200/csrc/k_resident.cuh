@@ -94,6 +94,14 @@ __device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v)
 }
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
+// q / d for the small operands of a CTA's staging loops: multiply-high by
+// m = floor((2^32 - 1) / d) + 1 is exact while q * d < 2^32; d = 1 (whose m
+// would not fit in 32 bits) is passed through.
+__host__ __device__ inline unsigned int div_magic(unsigned int d) { return d > 1u ? 0xffffffffu / d + 1u : 0u; }
+__device__ __forceinline__ unsigned int div_small(unsigned int q, unsigned int d, unsigned int m) {
+    return d > 1u ? __umulhi(q, m) : q;
+}
+
 // Grid-wide barrier of one cooperative launch, split into arrive and wait so
 // that a CTA can work between the two.  One 32-bit word counts the arrivals
 // of the launch: each CTA adds 1 per barrier with a release reduction (after
@@ -409,8 +417,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     const int KS = min(ks_fit, nk);
     auto defect_brick = [&]() {
         double* const P = reinterpret_cast<double*>(smem_raw);
-        // q / RW and row / RJ by multiply-high: exact while q * RW < 2^32
-        const unsigned int mRW = 0xffffffffu / (unsigned)RW + 1u, mRJ = 0xffffffffu / (unsigned)RJ + 1u;
+        const unsigned int mRW = div_magic(RW), mRJ = div_magic(RJ);
         for (int ks0 = 0; ks0 < nk; ks0 += KS) {
             const int kn = min(KS, nk - ks0);
             const int total = RJ * (kn + 2) * RW;
@@ -420,9 +427,9 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
 #pragma unroll
                 for (int u = 0; u < kStage; ++u) {
                     const unsigned int q = (unsigned)min(q0 + tid + NT * u, total - 1);
-                    const unsigned int row = __umulhi(q, mRW);           // q / RW
+                    const unsigned int row = div_small(q, RW, mRW);
                     const unsigned int i = q - row * (unsigned)RW;
-                    const unsigned int kk = __umulhi(row, mRJ);          // row / RJ
+                    const unsigned int kk = div_small(row, RJ, mRJ);
                     const unsigned int jj = row - kk * (unsigned)RJ;
                     v[u] = __ldcg(p + base + (long long)jj * g.px + (long long)kk * g.pz + i);
                 }
@@ -433,23 +440,39 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 }
             }
             __syncthreads();
-            for (int row = warp; row < nj * kn; row += NWARP) {
-                const int jl = row % nj + 1, kq = row / nj + 1;   // kq: plane of the slab (1..kn)
-                const int kl = ks0 + kq;
-                const int j = j0 + jl - 1, k = k0 + kl - 1;
-                const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-                const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
-                const long long g0 = spl(g, 0, j, k);
-                const long long c0 = nat(g, 0, j, k);
-                const double* Pr = P + (kq * RJ + jl) * RW;
-                for (int i = 1 + lane; i <= g.nx; i += 32) {
-                    const double dval = defect_value(g.cE[i], Pr[i + 1], g.cW[i], Pr[i - 1], cN, Pr[i + RW], cS,
-                                                     Pr[i - RW], cF, Pr[i + RJ * RW], cB, Pr[i - RJ * RW],
-                                                     __ldg(b + c0 + i), Pr[i]);
+            // the slab's cells in rounds of kStage per thread: the round's b' (the only
+            // operand in global memory) is loaded for every cell before any is formed
+            const int cells = nj * kn * g.nx;
+            const unsigned int mNX = div_magic(g.nx), mNJ = div_magic(nj);
+            for (int q0 = 0; q0 < cells; q0 += NT * kStage) {
+                double bv[kStage];
+                int ci[kStage], cr[kStage];
+#pragma unroll
+                for (int u = 0; u < kStage; ++u) {
+                    const unsigned int q = (unsigned)min(q0 + tid + NT * u, cells - 1);
+                    const unsigned int row = div_small(q, g.nx, mNX);
+                    ci[u] = (int)(q - row * (unsigned)g.nx) + 1;             // i
+                    cr[u] = (int)row;
+                    const unsigned int kq = div_small(row, nj, mNJ);
+                    const int jl = (int)(row - kq * (unsigned)nj) + 1;
+                    bv[u] = __ldg(b + nat(g, ci[u], j0 + jl - 1, k0 + ks0 + (int)kq));
+                }
+#pragma unroll
+                for (int u = 0; u < kStage; ++u) {
+                    if (q0 + tid + NT * u >= cells) continue;
+                    const int i = ci[u];
+                    const int kq = (int)div_small((unsigned)cr[u], nj, mNJ);
+                    const int jl = cr[u] - kq * nj + 1;
+                    const int kl = ks0 + kq + 1;
+                    const int j = j0 + jl - 1, k = k0 + kl - 1;
+                    const double* Pr = P + ((kq + 1) * RJ + jl) * RW;
+                    const double dval = defect_value(g.cE[i], Pr[i + 1], g.cW[i], Pr[i - 1], g.cN[j], Pr[i + RW],
+                                                     g.cS[j], Pr[i - RW], g.cF[k], Pr[i + RJ * RW], g.cB[k],
+                                                     Pr[i - RJ * RW], bv[u], Pr[i]);
                     const int m = (i + 2) >> 1;
                     const bool red = ((i + j + k) & 1) == 0;
-                    if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
-                    else (red ? dRg : dBg)[g0 + m] = (Tc)dval;
+                    if (CD) (red ? D0 : D1)[((kl - 1) * JB + (jl - 1)) * mx + m] = (Tc)dval;
+                    else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
                 }
             }
             __syncthreads();
