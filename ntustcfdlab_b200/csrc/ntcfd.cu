@@ -24,6 +24,7 @@
 #include "k_adjoint.cuh"
 #include "k_mask.cuh"
 #include "k_predictor.cuh"
+#include "k_predictor32.cuh"
 #include "k_schemes.cuh"
 #include "k_pressure.cuh"
 #include "k_project.cuh"
@@ -216,6 +217,13 @@ dim3 grid3(const Geom& g, dim3 b) {
     return dim3((g.nx + b.x - 1) / b.x, (g.ny + b.y - 1) / b.y, (g.nz + b.z - 1) / b.z);
 }
 
+// Launch shape of the FP32 predictor: 32 x 8 columns, chunks of kc planes;
+// the dynamic shared memory holds the chunk's z tables.
+dim3 p32_grid(const Geom& g, int kc) {
+    return dim3((g.nx + kP32BX - 1) / kP32BX, (g.ny + kP32BY - 1) / kP32BY, (g.nz + kc - 1) / kc);
+}
+size_t p32_smem(int kc) { return sizeof(float) * 6 * (size_t)(kc + 5); }
+
 // ---- graph construction helpers
 template <class Tuple, size_t... I>
 void fill_ptrs(Tuple& t, void** p, std::index_sequence<I...>) {
@@ -373,7 +381,10 @@ void launch_predictor(ntcfd_ctx* ctx, cudaStream_t st) {
                                          P.smag_mode == NTCFD_SMAG_REF_ALIASED ? 1 : 0);
     const PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
                       P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
-    if (qc) k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
+    if (qc && P.precision == NTCFD_MIXED) {
+        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->sm_count);
+        k_predictor32<<<p32_grid(g, kc), dim3(kP32BX, kP32BY), p32_smem(kc), st>>>(g, ctx->tpf, pa, kc);
+    } else if (qc) k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
     else if (P.scheme == NTCFD_QUICK) k_predictor_scheme<kSchemeQuick><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
     else if (P.scheme == NTCFD_UPWIND) k_predictor_scheme<kSchemeUpwind><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
     else k_predictor_scheme<kSchemeCentre><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
@@ -402,7 +413,11 @@ int build_graph(ntcfd_ctx* ctx) {
     }
     PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
                 P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
-    if (qc) GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
+    if (qc && P.precision == NTCFD_MIXED) {
+        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->sm_count);
+        GK(add_kernel_ex(&n, G, dep, k_predictor32, p32_grid(g, kc), dim3(kP32BX, kP32BY), p32_smem(kc), false,
+                         g, ctx->tpf, pa, kc));
+    } else if (qc) GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
     else if (P.scheme == NTCFD_QUICK)
         GK(add_kernel(&n, G, dep, k_predictor_scheme<kSchemeQuick>, g3, b3, g, ctx->tpd, pa, P.Cs));
     else if (P.scheme == NTCFD_UPWIND)
