@@ -61,17 +61,17 @@ __device__ __forceinline__ Tc sor_update(Tc cE, Tc oE, Tc cW, Tc oW, Tc cN, Tc o
 }
 
 // FP64 defect of a cell, d = rdiag * sum_nb c_nb p_nb - b' - p (the reference
-// sweep's fixed-point residual): the same sums as sor_update and rdiag_of.
+// sweep's fixed-point residual), rd = rdiag_of of the cell: the same sums as
+// sor_update.
 __device__ __forceinline__ double defect_value(double cE, double pe, double cW, double pw, double cN, double pn,
                                                double cS, double ps, double cF, double pf, double cB, double pb,
-                                               double bv, double pc) {
+                                               double rd, double bv, double pc) {
     double s = mul_rn(cE, pe);
     s = fma_rn(cW, pw, s);
     s = fma_rn(cN, pn, s);
     s = fma_rn(cS, ps, s);
     s = fma_rn(cF, pf, s);
     s = fma_rn(cB, pb, s);
-    const double rd = rcp_rn(((cE + cW) + (cN + cS)) + (cF + cB));
     return sub_rn(fma_rn(rd, s, -bv), pc);
 }
 
@@ -152,10 +152,22 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
     if (i > g.nx || j > g.ny || k > g.nz) return;
     const long long c = nat(g, i, j, k);
     const double d = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], sc.cN[j], p[c + g.px], sc.cS[j],
-                                  p[c - g.px], sc.cF[k], p[c + g.pz], sc.cB[k], p[c - g.pz], b[c], p[c]);
+                                  p[c - g.px], sc.cF[k], p[c + g.pz], sc.cB[k], p[c - g.pz], rdiag_of(sc, i, j, k),
+                                  b[c], p[c]);
     const long long q = spl(g, (i + 2) >> 1, j, k);
     if (((i + j + k) & 1) == 0) { dR[q] = (Tc)d; eR[q] = Tc(0); }
     else { dB[q] = (Tc)d; eB[q] = Tc(0); }
+}
+
+// The FP64 rdiag_of of every interior cell in the natural layout (Geom::rd64):
+// the defect passes of the resident kernel read it instead of forming the
+// reciprocal, with the same bits.
+__global__ void k_make_rd64(Geom g, SorCoef<double> sc, double* rd64) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    rd64[nat(g, i, j, k)] = rdiag_of(sc, i, j, k);
 }
 
 // rd = 1 / sum of the six coefficients of every interior cell, per colour,

@@ -20,7 +20,8 @@
 // e = 0.  A defect pass stages p of the brick and its ring in shared memory
 // (over the e tile, which is free then) a slab of planes at a time and forms
 // d = rdiag sum c p_nb - b' - p from there (defect_value, the arithmetic of
-// k_defect), so its loads are plain copies with many in flight.
+// k_defect, with rdiag from the grid's FP64 table); the staging is one bulk
+// (TMA) copy per row.
 //
 // A lane updates two cells at a time with every load issued before any
 // store: cells t and t + 32 of one row (rows of at most 64 cells per colour,
@@ -94,12 +95,42 @@ __device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v)
 }
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
-// q / d for the small operands of a CTA's staging loops: multiply-high by
-// m = floor((2^32 - 1) / d) + 1 is exact while q * d < 2^32; d = 1 (whose m
-// would not fit in 32 bits) is passed through.
-__host__ __device__ inline unsigned int div_magic(unsigned int d) { return d > 1u ? 0xffffffffu / d + 1u : 0u; }
-__device__ __forceinline__ unsigned int div_small(unsigned int q, unsigned int d, unsigned int m) {
-    return d > 1u ? __umulhi(q, m) : q;
+// Bulk (TMA) copies of whole rows from global to shared memory, completed on
+// an mbarrier.  A copy starts on 16-byte boundaries at both ends and moves a
+// multiple of 16 bytes; no cluster multicast.
+__device__ __forceinline__ unsigned int smem_u32(const void* q) {
+    return (unsigned int)__cvta_generic_to_shared(q);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned int bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned int parity) {
+    unsigned int ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+__device__ __forceinline__ void bulk_row_to_smem(void* dst, const void* src, unsigned int bytes,
+                                                 unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+// Orders this thread's generic-proxy accesses (shared memory, and global data
+// acquired from other CTAs) before the async-proxy copies it issues next.
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
 // Grid-wide barrier of one cooperative launch, split into arrive and wait so
@@ -264,6 +295,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     using B = decltype(abs_bits(Tc(0)));
     __shared__ int s_flag;
     __shared__ unsigned long long s_ring;
+    __shared__ __align__(8) unsigned long long s_mbar;   // completion of the staging copies
     __shared__ B s_red[NT / 32];
     const int JB = br.JB, KB = br.KB, mx = br.mx;
     const int RS = JB + 2;                    // rows per k-plane of the tile
@@ -305,6 +337,10 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     // cells of a colour in a row of parity r
     const int nown0 = g.nx / 2, nown1 = (g.nx + 1) / 2;
 
+    if (tid == 0) {
+        mbar_init(&s_mbar, 1u);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     for (int q = tid; q < 2 * tile; q += NT) S0[q] = Tc(0);
     for (int i = tid - 1; i <= g.nx + 2; i += NT) {
         cEs[i] = sc.cE[i];
@@ -409,72 +445,103 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
 
     // FP64 defect of the brick into D0/D1 (or the global d arrays), with p of the
     // brick and its one-row ring staged in shared memory over the e tile, a slab of
-    // KS planes at a time.  Every p is read through L2 (rows of other bricks were
-    // written by other SMs); every load of a staging round is issued before its
-    // stores.
-    const int RW = g.nx + 2, RJ = nj + 2;
-    const int ks_fit = (int)((2 * (size_t)tile * sizeof(Tc)) / ((size_t)RJ * RW * sizeof(double))) - 2;
+    // KS planes at a time: one bulk copy per row (i = -1 .. RWp-2; RWp even, so a
+    // row is a multiple of 16 bytes and starts 48 bytes into a 64-byte aligned
+    // global row), issued by warp 0 and completed on the mbarrier.  Then a warp
+    // takes two rows at a time, lanes along i, with the lane's cE, cW in registers
+    // and the rows' b' and 1/diag (Geom::rd64) loaded before any cell is formed.
+    const int RWp = (g.nx + 5) & ~1, RJ = nj + 2;
+    const int ks_fit = (int)((2 * (size_t)tile * sizeof(Tc)) / ((size_t)RJ * RWp * sizeof(double))) - 2;
     const int KS = min(ks_fit, nk);
+    unsigned int mphase = 0;
+    constexpr int DU = 2;   // cells per lane per row and i-chunk
+    auto defect_cells = [&](int rows, auto&& rowpos, auto&& pval) {
+        // rows of the pass: rowpos(r, jl, kl, kq) gives the row's brick position and
+        // its plane in the staged slab; pval(kq, jl, i, di, dj, dk) reads p
+        for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
+            double ce[DU], cw[DU];
+#pragma unroll
+            for (int u = 0; u < DU; ++u) {
+                const int i = min(ic + lane + 32 * u, g.nx);
+                ce[u] = g.cE[i];
+                cw[u] = g.cW[i];
+            }
+            for (int r0 = warp; r0 < rows; r0 += 2 * NWARP) {
+                double bv[2][DU], rv[2][DU];
+                int jl[2], kl[2], kq[2];
+                long long c0[2];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = min(r0 + h * NWARP, rows - 1);
+                    rowpos(r, jl[h], kl[h], kq[h]);
+                    c0[h] = nat(g, 0, j0 + jl[h] - 1, k0 + kl[h] - 1);
+#pragma unroll
+                    for (int u = 0; u < DU; ++u) {
+                        const int i = min(ic + lane + 32 * u, g.nx);
+                        bv[h][u] = __ldg(b + c0[h] + i);
+                        rv[h][u] = __ldg(g.rd64 + c0[h] + i);
+                    }
+                }
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    if (r0 + h * NWARP >= rows) continue;
+                    const int j = j0 + jl[h] - 1, k = k0 + kl[h] - 1;
+                    const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
+                    const int dr = ((kl[h] - 1) * JB + (jl[h] - 1)) * mx;
+#pragma unroll
+                    for (int u = 0; u < DU; ++u) {
+                        const int i = ic + lane + 32 * u;
+                        if (i > g.nx) continue;
+                        const int q = kq[h], y = jl[h];
+                        const double dval = defect_value(ce[u], pval(q, y, i, 1, 0, 0), cw[u], pval(q, y, i, -1, 0, 0),
+                                                         cN, pval(q, y, i, 0, 1, 0), cS, pval(q, y, i, 0, -1, 0), cF,
+                                                         pval(q, y, i, 0, 0, 1), cB, pval(q, y, i, 0, 0, -1), rv[h][u],
+                                                         bv[h][u], pval(q, y, i, 0, 0, 0));
+                        const int m = (i + 2) >> 1;
+                        const bool red = ((i + j + k) & 1) == 0;
+                        if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
+                        else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
+                    }
+                }
+            }
+        }
+    };
     auto defect_brick = [&]() {
         double* const P = reinterpret_cast<double*>(smem_raw);
-        const unsigned int mRW = div_magic(RW), mRJ = div_magic(RJ);
         for (int ks0 = 0; ks0 < nk; ks0 += KS) {
             const int kn = min(KS, nk - ks0);
-            const int total = RJ * (kn + 2) * RW;
-            const long long base = nat(g, 0, j0 - 1, k0 + ks0 - 1);
-            for (int q0 = 0; q0 < total; q0 += NT * kStage) {
-                double v[kStage];
-#pragma unroll
-                for (int u = 0; u < kStage; ++u) {
-                    const unsigned int q = (unsigned)min(q0 + tid + NT * u, total - 1);
-                    const unsigned int row = div_small(q, RW, mRW);
-                    const unsigned int i = q - row * (unsigned)RW;
-                    const unsigned int kk = div_small(row, RJ, mRJ);
-                    const unsigned int jj = row - kk * (unsigned)RJ;
-                    v[u] = __ldcg(p + base + (long long)jj * g.px + (long long)kk * g.pz + i);
-                }
-#pragma unroll
-                for (int u = 0; u < kStage; ++u) {
-                    const int q = q0 + tid + NT * u;
-                    if (q < total) P[q] = v[u];
-                }
-            }
+            const int nrow = RJ * (kn + 2);
+            // the tile was read and written through the generic proxy: order that
+            // before the copies overwrite it
+            fence_proxy_async();
             __syncthreads();
-            // the slab's cells in rounds of kStage per thread: the round's b' (the only
-            // operand in global memory) is loaded for every cell before any is formed
-            const int cells = nj * kn * g.nx;
-            const unsigned int mNX = div_magic(g.nx), mNJ = div_magic(nj);
-            for (int q0 = 0; q0 < cells; q0 += NT * kStage) {
-                double bv[kStage];
-                int ci[kStage], cr[kStage];
-#pragma unroll
-                for (int u = 0; u < kStage; ++u) {
-                    const unsigned int q = (unsigned)min(q0 + tid + NT * u, cells - 1);
-                    const unsigned int row = div_small(q, g.nx, mNX);
-                    ci[u] = (int)(q - row * (unsigned)g.nx) + 1;             // i
-                    cr[u] = (int)row;
-                    const unsigned int kq = div_small(row, nj, mNJ);
-                    const int jl = (int)(row - kq * (unsigned)nj) + 1;
-                    bv[u] = __ldg(b + nat(g, ci[u], j0 + jl - 1, k0 + ks0 + (int)kq));
-                }
-#pragma unroll
-                for (int u = 0; u < kStage; ++u) {
-                    if (q0 + tid + NT * u >= cells) continue;
-                    const int i = ci[u];
-                    const int kq = (int)div_small((unsigned)cr[u], nj, mNJ);
-                    const int jl = cr[u] - kq * nj + 1;
-                    const int kl = ks0 + kq + 1;
-                    const int j = j0 + jl - 1, k = k0 + kl - 1;
-                    const double* Pr = P + ((kq + 1) * RJ + jl) * RW;
-                    const double dval = defect_value(g.cE[i], Pr[i + 1], g.cW[i], Pr[i - 1], g.cN[j], Pr[i + RW],
-                                                     g.cS[j], Pr[i - RW], g.cF[k], Pr[i + RJ * RW], g.cB[k],
-                                                     Pr[i - RJ * RW], bv[u], Pr[i]);
-                    const int m = (i + 2) >> 1;
-                    const bool red = ((i + j + k) & 1) == 0;
-                    if (CD) (red ? D0 : D1)[((kl - 1) * JB + (jl - 1)) * mx + m] = (Tc)dval;
-                    else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
+            if (warp == 0) {
+                if (lane == 0) mbar_arrive_expect_tx(&s_mbar, (unsigned)(nrow * RWp * sizeof(double)));
+                __syncwarp();
+                for (int row = lane; row < nrow; row += 32) {
+                    const int kk = row / RJ, jj = row - kk * RJ;
+                    bulk_row_to_smem(P + (size_t)row * RWp, p + nat(g, -1, j0 - 1 + jj, k0 + ks0 - 1 + kk),
+                                     (unsigned)(RWp * sizeof(double)), &s_mbar);
                 }
             }
+            // bounded wait for the slab (the copies are issued above, so it ends)
+            unsigned int polls = 0;
+            while (!mbar_try_wait(&s_mbar, mphase)) {
+                if (++polls > kBarrierPolls) {
+                    if (tid == 0) atomicExch(&bar->err, 1);
+                    break;
+                }
+            }
+            mphase ^= 1u;
+            defect_cells(nj * kn,
+                         [&](int r, int& jl, int& kl, int& kq) {
+                             kq = r / nj;
+                             jl = r - kq * nj + 1;
+                             kl = ks0 + kq + 1;
+                         },
+                         [&](int q, int y, int i, int di, int dj, int dk) {
+                             return P[((q + 1 + dk) * RJ + y + dj) * RWp + (i + 1 + di)];
+                         });
             __syncthreads();
         }
     };
@@ -482,29 +549,20 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     // stage a slab): rows of this brick (and the frozen ghosts) through L1, this CTA
     // wrote them; rows of the neighbour bricks, written by other SMs, from L2 only.
     auto defect_direct = [&]() {
-        for (int row = warp; row < nrows; row += NWARP) {
-            const int jl = row % nj + 1, kl = row / nj + 1;
-            const int j = j0 + jl - 1, k = k0 + kl - 1;
-            const long long c0 = nat(g, 0, j, k);
-            const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
-            const long long g0 = spl(g, 0, j, k);
-            const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-            const bool nL1 = jl < nj || j == g.ny, sL1 = jl > 1 || j == 1;
-            const bool fL1 = kl < nk || k == g.nz, bL1 = kl > 1 || k == 1;
-            for (int i = 1 + lane; i <= g.nx; i += 32) {
-                const long long c = c0 + i;
-                const double pn = nL1 ? __ldca(p + c + g.px) : __ldcg(p + c + g.px);
-                const double ps = sL1 ? __ldca(p + c - g.px) : __ldcg(p + c - g.px);
-                const double pf = fL1 ? __ldca(p + c + g.pz) : __ldcg(p + c + g.pz);
-                const double pb = bL1 ? __ldca(p + c - g.pz) : __ldcg(p + c - g.pz);
-                const double dval = defect_value(g.cE[i], __ldca(p + c + 1), g.cW[i], __ldca(p + c - 1), cN, pn, cS,
-                                                 ps, cF, pf, cB, pb, __ldg(b + c), __ldca(p + c));
-                const int m = (i + 2) >> 1;
-                const bool red = ((i + j + k) & 1) == 0;
-                if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
-                else (red ? dRg : dBg)[g0 + m] = (Tc)dval;
-            }
-        }
+        defect_cells(nrows,
+                     [&](int r, int& jl, int& kl, int& kq) {
+                         kq = 0;
+                         jl = r % nj + 1;
+                         kl = r / nj + 1;
+                         kq = kl;   // carries kl to pval
+                     },
+                     [&](int kls, int jl, int i, int di, int dj, int dk) {
+                         const int j = j0 + jl - 1, k = k0 + kls - 1;
+                         const bool own = (jl + dj >= 1 && jl + dj <= nj) || j + dj < 1 || j + dj > g.ny;
+                         const bool ownk = (kls + dk >= 1 && kls + dk <= nk) || k + dk < 1 || k + dk > g.nz;
+                         const double* q = p + nat(g, i + di, j + dj, k + dk);
+                         return (own && ownk) ? __ldca(q) : __ldcg(q);
+                     });
         __syncthreads();
     };
     // the published boundary rows of e, both colours, to zero

@@ -84,6 +84,7 @@ struct ntcfd_ctx {
     double *us = nullptr, *vs = nullptr, *ws = nullptr, *b = nullptr;
     double *eta = nullptr, *nut = nullptr;
     double* fb = nullptr;                   // body force fu, fv, fw (3 natural arrays), null when unset
+    double* rd64 = nullptr;                 // FP64 1/diag of every cell (natural layout)
     void *eR = nullptr, *eB = nullptr, *dR = nullptr, *dB = nullptr;
     void *rdR = nullptr, *rdB = nullptr;   // 1/diag per colour (sweep precision)
     double* tabd = nullptr;   // double tables
@@ -850,7 +851,8 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
     ctx->spl_elems = (size_t)g.mz * (P.nz + 4);
     const size_t N = ctx->nat_elems;
     int rc;
-    double** nat[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->us, &ctx->vs, &ctx->ws, &ctx->b, &ctx->eta};
+    double** nat[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->us, &ctx->vs, &ctx->ws, &ctx->b, &ctx->eta,
+                      &ctx->rd64};
     for (double** a : nat)
         if ((rc = dalloc(ctx, a, N))) return rc;
     if (P.LES && (rc = dalloc(ctx, &ctx->nut, N))) return rc;
@@ -992,6 +994,8 @@ int ntcfd_set_metrics(ntcfd_ctx* ctx, const double* iDx, const double* Dxs, cons
     }
     {
         const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+        g.rd64 = ctx->rd64;
+        k_make_rd64<<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->rd64);
         if (ctx->prm.precision == NTCFD_MIXED)
             k_make_rd<float><<<g3, b3, 0, ctx->stream>>>(g, ctx->scf, (float*)ctx->rdR, (float*)ctx->rdB);
         else
