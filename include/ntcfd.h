@@ -86,7 +86,7 @@ typedef struct ntcfd_params {
     double bc_value[6][3];   /* Dirichlet value (the reference hard-codes 1.0) */
     double u_solid[3];       /* solid velocity in the forcing (variables_module.f90:331-335) */
     double lx;               /* force-coefficient normalisation (virtualForceIntegrator.f90:80-81) */
-    int mixed_cycle;         /* MIXED: max FP32 sweeps per defect-correction cycle (0 = itmax) */
+    int mixed_cycle;         /* sweeps per defect-correction cycle; 0: 8 for MIXED, itmax for FP64 */
     int diag_divergence;     /* 1: report max|div u^{n+1}| in ntcfd_step_info.div_max */
     int device;              /* CUDA device ordinal that holds the grid */
     int sor_path;            /* NTCFD_SOR_AUTO, NTCFD_SOR_STREAMING or NTCFD_SOR_RESIDENT */

@@ -159,17 +159,6 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
     else { dB[q] = (Tc)d; eB[q] = Tc(0); }
 }
 
-// The FP64 rdiag_of of every interior cell in the natural layout (Geom::rd64):
-// the defect passes of the resident kernel read it instead of forming the
-// reciprocal, with the same bits.
-__global__ void k_make_rd64(Geom g, SorCoef<double> sc, double* rd64) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
-    if (i > g.nx || j > g.ny || k > g.nz) return;
-    rd64[nat(g, i, j, k)] = rdiag_of(sc, i, j, k);
-}
-
 // rd = 1 / sum of the six coefficients of every interior cell, per colour,
 // in the sweeps' precision; it depends on the grid only and is made once.
 template <class Tc>

@@ -20,8 +20,7 @@
 // e = 0.  A defect pass stages p of the brick and its ring in shared memory
 // (over the e tile, which is free then) a slab of planes at a time and forms
 // d = rdiag sum c p_nb - b' - p from there (defect_value, the arithmetic of
-// k_defect, with rdiag from the grid's FP64 table); the staging is one bulk
-// (TMA) copy per row.
+// k_defect); the staging is one bulk (TMA) copy per row of p and b'.
 //
 // A lane updates two cells at a time with every load issued before any
 // store: cells t and t + 32 of one row (rows of at most 64 cells per colour,
@@ -444,84 +443,45 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     };
 
     // FP64 defect of the brick into D0/D1 (or the global d arrays), with p of the
-    // brick and its one-row ring staged in shared memory over the e tile, a slab of
-    // KS planes at a time: one bulk copy per row (i = -1 .. RWp-2; RWp even, so a
-    // row is a multiple of 16 bytes and starts 48 bytes into a 64-byte aligned
-    // global row), issued by warp 0 and completed on the mbarrier.  Then a warp
-    // takes two rows at a time, lanes along i, with the lane's cE, cW in registers
-    // and the rows' b' and 1/diag (Geom::rd64) loaded before any cell is formed.
-    const int RWp = (g.nx + 5) & ~1, RJ = nj + 2;
-    const int ks_fit = (int)((2 * (size_t)tile * sizeof(Tc)) / ((size_t)RJ * RWp * sizeof(double))) - 2;
+    // brick and its one-row ring and b' of the brick staged in shared memory over
+    // the e tile, a slab of KS planes at a time: one bulk copy per row, issued by
+    // warp 0 and completed on the mbarrier.  A p row holds i = -1 .. RWp-2 (RWp
+    // even: a multiple of 16 bytes, starting 48 bytes into a 64-byte aligned global
+    // row), a b' row i = 1 .. RWb (RWb even, 64-byte aligned start).  Then a warp
+    // takes the slab's rows, lanes along i, with the lane's cE, cW in registers;
+    // every operand of a cell is in shared memory, and rdiag is formed as rdiag_of
+    // forms it.
+    const int RWp = (g.nx + 5) & ~1, RWb = (g.nx + 1) & ~1, RJ = nj + 2;
+    const size_t stage_bytes = 2 * (size_t)tile * sizeof(Tc);
+    const int ks_fit = (int)((stage_bytes - 2 * (size_t)RJ * RWp * sizeof(double)) /
+                             (((size_t)RJ * RWp + (size_t)nj * RWb) * sizeof(double)));
     const int KS = min(ks_fit, nk);
     unsigned int mphase = 0;
-    constexpr int DU = 2;   // cells per lane per row and i-chunk
-    auto defect_cells = [&](int rows, auto&& rowpos, auto&& pval) {
-        // rows of the pass: rowpos(r, jl, kl, kq) gives the row's brick position and
-        // its plane in the staged slab; pval(kq, jl, i, di, dj, dk) reads p
-        for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
-            double ce[DU], cw[DU];
-#pragma unroll
-            for (int u = 0; u < DU; ++u) {
-                const int i = min(ic + lane + 32 * u, g.nx);
-                ce[u] = g.cE[i];
-                cw[u] = g.cW[i];
-            }
-            for (int r0 = warp; r0 < rows; r0 += 2 * NWARP) {
-                double bv[2][DU], rv[2][DU];
-                int jl[2], kl[2], kq[2];
-                long long c0[2];
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int r = min(r0 + h * NWARP, rows - 1);
-                    rowpos(r, jl[h], kl[h], kq[h]);
-                    c0[h] = nat(g, 0, j0 + jl[h] - 1, k0 + kl[h] - 1);
-#pragma unroll
-                    for (int u = 0; u < DU; ++u) {
-                        const int i = min(ic + lane + 32 * u, g.nx);
-                        bv[h][u] = __ldg(b + c0[h] + i);
-                        rv[h][u] = __ldg(g.rd64 + c0[h] + i);
-                    }
-                }
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    if (r0 + h * NWARP >= rows) continue;
-                    const int j = j0 + jl[h] - 1, k = k0 + kl[h] - 1;
-                    const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-                    const int dr = ((kl[h] - 1) * JB + (jl[h] - 1)) * mx;
-#pragma unroll
-                    for (int u = 0; u < DU; ++u) {
-                        const int i = ic + lane + 32 * u;
-                        if (i > g.nx) continue;
-                        const int q = kq[h], y = jl[h];
-                        const double dval = defect_value(ce[u], pval(q, y, i, 1, 0, 0), cw[u], pval(q, y, i, -1, 0, 0),
-                                                         cN, pval(q, y, i, 0, 1, 0), cS, pval(q, y, i, 0, -1, 0), cF,
-                                                         pval(q, y, i, 0, 0, 1), cB, pval(q, y, i, 0, 0, -1), rv[h][u],
-                                                         bv[h][u], pval(q, y, i, 0, 0, 0));
-                        const int m = (i + 2) >> 1;
-                        const bool red = ((i + j + k) & 1) == 0;
-                        if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
-                        else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
-                    }
-                }
-            }
-        }
-    };
+    constexpr int DU = 4;   // cells per lane per row and i-chunk
     auto defect_brick = [&]() {
         double* const P = reinterpret_cast<double*>(smem_raw);
         for (int ks0 = 0; ks0 < nk; ks0 += KS) {
             const int kn = min(KS, nk - ks0);
-            const int nrow = RJ * (kn + 2);
+            const int nrow = RJ * (kn + 2), nbrow = nj * kn;
+            double* const Bs = P + (size_t)nrow * RWp;
             // the tile was read and written through the generic proxy: order that
             // before the copies overwrite it
             fence_proxy_async();
             __syncthreads();
             if (warp == 0) {
-                if (lane == 0) mbar_arrive_expect_tx(&s_mbar, (unsigned)(nrow * RWp * sizeof(double)));
+                if (lane == 0)
+                    mbar_arrive_expect_tx(&s_mbar, (unsigned)(((size_t)nrow * RWp + (size_t)nbrow * RWb) * sizeof(double)));
                 __syncwarp();
-                for (int row = lane; row < nrow; row += 32) {
-                    const int kk = row / RJ, jj = row - kk * RJ;
-                    bulk_row_to_smem(P + (size_t)row * RWp, p + nat(g, -1, j0 - 1 + jj, k0 + ks0 - 1 + kk),
-                                     (unsigned)(RWp * sizeof(double)), &s_mbar);
+                for (int row = lane; row < nrow + nbrow; row += 32) {
+                    if (row < nrow) {
+                        const int kk = row / RJ, jj = row - kk * RJ;
+                        bulk_row_to_smem(P + (size_t)row * RWp, p + nat(g, -1, j0 - 1 + jj, k0 + ks0 - 1 + kk),
+                                         (unsigned)(RWp * sizeof(double)), &s_mbar);
+                    } else {
+                        const int r = row - nrow, kq = r / nj, jl = r - kq * nj;
+                        bulk_row_to_smem(Bs + (size_t)r * RWb, b + nat(g, 1, j0 + jl, k0 + ks0 + kq),
+                                         (unsigned)(RWb * sizeof(double)), &s_mbar);
+                    }
                 }
             }
             // bounded wait for the slab (the copies are issued above, so it ends)
@@ -533,36 +493,70 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                 }
             }
             mphase ^= 1u;
-            defect_cells(nj * kn,
-                         [&](int r, int& jl, int& kl, int& kq) {
-                             kq = r / nj;
-                             jl = r - kq * nj + 1;
-                             kl = ks0 + kq + 1;
-                         },
-                         [&](int q, int y, int i, int di, int dj, int dk) {
-                             return P[((q + 1 + dk) * RJ + y + dj) * RWp + (i + 1 + di)];
-                         });
+            for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
+                double ce[DU], cw[DU];
+#pragma unroll
+                for (int u = 0; u < DU; ++u) {
+                    const int i = min(ic + lane + 32 * u, g.nx);
+                    ce[u] = g.cE[i];
+                    cw[u] = g.cW[i];
+                }
+                for (int r = warp; r < nbrow; r += NWARP) {
+                    const int kq = r / nj, jl = r - kq * nj + 1;
+                    const int kl = ks0 + kq + 1;
+                    const int j = j0 + jl - 1, k = k0 + kl - 1;
+                    const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
+                    const double sNS = cN + cS, sFB = cF + cB;
+                    const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
+                    const double* Pr = P + (size_t)((kq + 1) * RJ + jl) * RWp + 1;   // Pr[i]: p(i, j, k)
+                    const double* Br = Bs + (size_t)r * RWb - 1;                     // Br[i]: b'(i, j, k)
+#pragma unroll
+                    for (int u = 0; u < DU; ++u) {
+                        const int i = ic + lane + 32 * u;
+                        if (i > g.nx) continue;
+                        const double rd = rcp_rn(((ce[u] + cw[u]) + sNS) + sFB);
+                        const double dval =
+                            defect_value(ce[u], Pr[i + 1], cw[u], Pr[i - 1], cN, Pr[i + RWp], cS, Pr[i - RWp], cF,
+                                         Pr[i + RJ * RWp], cB, Pr[i - RJ * RWp], rd, Br[i], Pr[i]);
+                        const int m = (i + 2) >> 1;
+                        const bool red = ((i + j + k) & 1) == 0;
+                        if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
+                        else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
+                    }
+                }
+            }
             __syncthreads();
         }
     };
-    // The same defect with every p read from global memory (for tiles too small to
-    // stage a slab): rows of this brick (and the frozen ghosts) through L1, this CTA
-    // wrote them; rows of the neighbour bricks, written by other SMs, from L2 only.
+    // The same defect with every operand read from global memory (for tiles too
+    // small to stage a slab): rows of this brick (and the frozen ghosts) through L1,
+    // this CTA wrote them; rows of the neighbour bricks, written by other SMs, from
+    // L2 only.
     auto defect_direct = [&]() {
-        defect_cells(nrows,
-                     [&](int r, int& jl, int& kl, int& kq) {
-                         kq = 0;
-                         jl = r % nj + 1;
-                         kl = r / nj + 1;
-                         kq = kl;   // carries kl to pval
-                     },
-                     [&](int kls, int jl, int i, int di, int dj, int dk) {
-                         const int j = j0 + jl - 1, k = k0 + kls - 1;
-                         const bool own = (jl + dj >= 1 && jl + dj <= nj) || j + dj < 1 || j + dj > g.ny;
-                         const bool ownk = (kls + dk >= 1 && kls + dk <= nk) || k + dk < 1 || k + dk > g.nz;
-                         const double* q = p + nat(g, i + di, j + dj, k + dk);
-                         return (own && ownk) ? __ldca(q) : __ldcg(q);
-                     });
+        for (int row = warp; row < nrows; row += NWARP) {
+            const int jl = row % nj + 1, kl = row / nj + 1;
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const long long c0 = nat(g, 0, j, k);
+            const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
+            const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
+            const bool nL1 = jl < nj || j == g.ny, sL1 = jl > 1 || j == 1;
+            const bool fL1 = kl < nk || k == g.nz, bL1 = kl > 1 || k == 1;
+            for (int i = 1 + lane; i <= g.nx; i += 32) {
+                const long long c = c0 + i;
+                const double pn = nL1 ? __ldca(p + c + g.px) : __ldcg(p + c + g.px);
+                const double ps = sL1 ? __ldca(p + c - g.px) : __ldcg(p + c - g.px);
+                const double pf = fL1 ? __ldca(p + c + g.pz) : __ldcg(p + c + g.pz);
+                const double pb = bL1 ? __ldca(p + c - g.pz) : __ldcg(p + c - g.pz);
+                const double ce = g.cE[i], cw = g.cW[i];
+                const double rd = rcp_rn(((ce + cw) + (cN + cS)) + (cF + cB));
+                const double dval = defect_value(ce, __ldca(p + c + 1), cw, __ldca(p + c - 1), cN, pn, cS, ps, cF,
+                                                 pf, cB, pb, rd, __ldg(b + c), __ldca(p + c));
+                const int m = (i + 2) >> 1;
+                const bool red = ((i + j + k) & 1) == 0;
+                if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
+                else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
+            }
+        }
         __syncthreads();
     };
     // the published boundary rows of e, both colours, to zero

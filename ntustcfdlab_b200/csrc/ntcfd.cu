@@ -41,6 +41,7 @@ constexpr int kSweepBx = 64;     // column form: threads per row, rows per CTA, 
 constexpr int kSweepBy = 4;
 constexpr int kSweepKpt = 4;
 constexpr int kResNT = 512;      // threads per CTA of the resident SOR kernel
+constexpr int kMixedCycle = 8;   // default FP32 sweeps per defect-correction cycle (mixed_cycle = 0)
 const double kZeroZeta = 0.0;
 const int kOne = 1;
 
@@ -84,7 +85,6 @@ struct ntcfd_ctx {
     double *us = nullptr, *vs = nullptr, *ws = nullptr, *b = nullptr;
     double *eta = nullptr, *nut = nullptr;
     double* fb = nullptr;                   // body force fu, fv, fw (3 natural arrays), null when unset
-    double* rd64 = nullptr;                 // FP64 1/diag of every cell (natural layout)
     void *eR = nullptr, *eB = nullptr, *dR = nullptr, *dB = nullptr;
     void *rdR = nullptr, *rdB = nullptr;   // 1/diag per colour (sweep precision)
     double* tabd = nullptr;   // double tables
@@ -832,8 +832,11 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
     ntcfd_params& P = ctx->prm;
     if (P.check_every == 0) P.check_every = 1;
     ctx->csweeps = P.check_every;
-    int cl = P.mixed_cycle > 0 ? P.mixed_cycle : P.itmax;
-    if (P.mixed_cycle > 0 && cl % ctx->csweeps) cl += ctx->csweeps - cl % ctx->csweeps;
+    // sweeps per defect-correction cycle: mixed_cycle when set, else kMixedCycle for
+    // MIXED (FP32 sweeps) and one cycle for FP64
+    const bool cycles = P.mixed_cycle > 0 || P.precision == NTCFD_MIXED;
+    int cl = P.mixed_cycle > 0 ? P.mixed_cycle : (P.precision == NTCFD_MIXED ? kMixedCycle : P.itmax);
+    if (cycles && cl % ctx->csweeps) cl += ctx->csweeps - cl % ctx->csweeps;
     ctx->cycle_len = cl > 0 ? cl : 1;
     *out = ctx;
     CK(cudaSetDevice(P.device));
@@ -851,8 +854,7 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
     ctx->spl_elems = (size_t)g.mz * (P.nz + 4);
     const size_t N = ctx->nat_elems;
     int rc;
-    double** nat[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->us, &ctx->vs, &ctx->ws, &ctx->b, &ctx->eta,
-                      &ctx->rd64};
+    double** nat[] = {&ctx->u, &ctx->v, &ctx->w, &ctx->p, &ctx->us, &ctx->vs, &ctx->ws, &ctx->b, &ctx->eta};
     for (double** a : nat)
         if ((rc = dalloc(ctx, a, N))) return rc;
     if (P.LES && (rc = dalloc(ctx, &ctx->nut, N))) return rc;
@@ -994,8 +996,6 @@ int ntcfd_set_metrics(ntcfd_ctx* ctx, const double* iDx, const double* Dxs, cons
     }
     {
         const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
-        g.rd64 = ctx->rd64;
-        k_make_rd64<<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->rd64);
         if (ctx->prm.precision == NTCFD_MIXED)
             k_make_rd<float><<<g3, b3, 0, ctx->stream>>>(g, ctx->scf, (float*)ctx->rdR, (float*)ctx->rdB);
         else

@@ -39,9 +39,6 @@ struct Geom {
     //   cE(i) = 1/(iDx(i) Dxs(i)), cW(i) = 1/(iDx(i) Dxs(i-1)), likewise N/S, F/B
     const double *cE, *cW, *cN, *cS, *cF, *cB;
     const float *cEf, *cWf, *cNf, *cSf, *cFf, *cBf;
-    // 1 / sum of the six coefficients of every interior cell, FP64, natural layout
-    // (rdiag_of of k_pressure.cuh, made once per grid)
-    const double* rd64;
 };
 
 __host__ __device__ __forceinline__ long long nat(const Geom& g, int i, int j, int k) {
