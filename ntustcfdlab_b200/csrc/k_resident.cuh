@@ -75,14 +75,16 @@ inline size_t resident_smem(const Brick& b, int nx) {
     const size_t brick = (size_t)b.JB * b.KB * b.mx;
     const size_t arrays = sizeof(Tc) * (2 * tile + 2 * (size_t)(nx + 4) + 2 * (size_t)(b.JB + b.KB) +
                                         (b.cache_d ? 2 * brick : 0) + (b.cache_rd ? 2 * brick : 0));
-    // + row table (int4 offsets and four coefficients per row), + slack: the loads of
-    // a lane past a row's last cell may reach up to 64 elements beyond the tiles
+    // + row table (int4 offsets and four coefficients per row), + the face-ring list
+    // (int2 per ring row), + slack: the loads of a lane past a row's last cell may
+    // reach up to 64 elements beyond the tiles
     const size_t rows = (size_t)b.JB * b.KB;
-    return ((arrays + 15) & ~size_t(15)) + rows * (16 + 4 * sizeof(Tc)) + 64 * sizeof(Tc);
+    return ((arrays + 15) & ~size_t(15)) + rows * (16 + 4 * sizeof(Tc)) + 2 * (size_t)(b.JB + b.KB) * 8 +
+           64 * sizeof(Tc);
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
-constexpr int kStage = 8;                           // loads in flight per thread when staging p
+constexpr int kFill = 8;                            // loads in flight per thread when filling the ring
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -227,7 +229,7 @@ struct ResRow {
     const Tc* D;      // d of the row: brick row start (shared) or global row start
     const Tc* R;      // rd of the row, likewise
     Tc cN, cS, cF, cB;
-    int far;          // bits 2, 4, 8, 16: the N, S, F, B neighbour row lies in another brick
+    int par;          // (j + k) & 1 of the row
     long long gr;     // global colour-split row start
 };
 
@@ -237,30 +239,20 @@ struct ResIn {
     Tc oE, oW, oN, oS, oF, oB, e0, d, rd;
 };
 
-// Loads of the cell at own index m (t + 2 - R) of a row of parity R.  An
-// EDGE row reads a neighbour row that lies in another brick from the global
-// array Og (written by that brick's CTA before the last grid barrier, so
-// through L2: ld.global.cg).  d may be rewritten inside the launch by this
-// CTA only: a plain (L1-coherent) load when it is global.
-template <class Tc, bool CD, bool CR, bool EDGE, int R>
-__device__ __forceinline__ ResIn<Tc> res_load(const ResRow<Tc>& w, int m, int mx, int plane, const Tc* Og,
-                                              int ys, int zs) {
+// Loads of the cell at own index m (t + 2 - R) of a row of parity R, all from
+// shared memory: the tile's face ring holds the neighbour bricks' rows of the
+// other colour (fill_ring).  d may be rewritten inside the launch by this CTA
+// only: a plain (L1-coherent) load when it is global.
+template <class Tc, bool CD, bool CR, int R>
+__device__ __forceinline__ ResIn<Tc> res_load(const ResRow<Tc>& w, int m, int mx, int plane) {
     ResIn<Tc> x;
     const Tc* o = w.O + m;
     x.oE = o[R];
     x.oW = o[R - 1];
-    if (EDGE) {
-        const Tc* og = Og + w.gr + m;
-        x.oN = (w.far & 2) ? __ldcg(og + ys) : o[mx];
-        x.oS = (w.far & 4) ? __ldcg(og - ys) : o[-mx];
-        x.oF = (w.far & 8) ? __ldcg(og + zs) : o[plane];
-        x.oB = (w.far & 16) ? __ldcg(og - zs) : o[-plane];
-    } else {
-        x.oN = o[mx];
-        x.oS = o[-mx];
-        x.oF = o[plane];
-        x.oB = o[-plane];
-    }
+    x.oN = o[mx];
+    x.oS = o[-mx];
+    x.oF = o[plane];
+    x.oB = o[-plane];
     x.e0 = w.W[m];
     x.d = CD ? w.D[m] : __ldca(w.D + m);
     x.rd = CR ? w.R[m] : __ldg(w.R + m);
@@ -318,12 +310,14 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     Tc* const R1 = R0 + brick;
     Tc* const arrays_end = CR ? R1 + brick : (CD ? D1 + brick : D0);
     // row table: per row of the brick, in sweep order (edge rows first), the tile row
-    // start, the brick row start of d/rd, the global colour-split row start, and
-    // (j+k)&1 plus the bits of the neighbour rows in another brick; and the row's
-    // cN, cS, cF, cB
+    // start, the brick row start of d/rd, the global colour-split row start and
+    // (j+k)&1; and the row's cN, cS, cF, cB.  Then the face ring: per ring row of
+    // the tile that stands for a row of a neighbour brick, its tile row start and
+    // global colour-split row start (y = -1: a domain ghost row, kept at 0).
     const size_t toff = ((size_t)((unsigned char*)arrays_end - smem_raw) + 15) & ~size_t(15);
     int4* const rowT = reinterpret_cast<int4*>(smem_raw + toff);
     Tc* const rowC = reinterpret_cast<Tc*>(rowT + JB * KB);
+    int2* const ringT = reinterpret_cast<int2*>(rowC + 4 * JB * KB);
     constexpr int NWARP = NT / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tid = threadIdx.x;
@@ -358,14 +352,28 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     const int nrows = nj * nk;
     const int ni = (nj > 2 && nk > 2) ? (nj - 2) * (nk - 2) : 0;   // interior rows
     const int ne = nrows - ni;                                       // edge rows
+    const int nring = 2 * (nj + nk);
+    for (int q = tid; q < nring; q += NT) {
+        // faces j-low, j-high (nk rows each), then k-low, k-high (nj rows each)
+        int jl, kl;
+        if (q < 2 * nk) {
+            kl = q % nk + 1;
+            jl = q < nk ? 0 : nj + 1;
+        } else {
+            const int r = q - 2 * nk;
+            jl = r % nj + 1;
+            kl = r < nj ? 0 : nk + 1;
+        }
+        const int j = j0 + jl - 1, k = k0 + kl - 1;
+        const bool inner = j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
+        ringT[q] = make_int2((kl * RS + jl) * mx, inner ? ys * (j + 1) + zs * (k + 1) : -1);
+    }
     for (int er = tid; er < nrows; er += NT) {
         int jl, kl;
         brick_row(er, nj, nk, ni, ne, jl, kl);
         const int j = j0 + jl - 1, k = k0 + kl - 1;
-        const int far = (jl == nj && j < g.ny ? 2 : 0) | (jl == 1 && j > 1 ? 4 : 0) |
-                        (kl == nk && k < g.nz ? 8 : 0) | (kl == 1 && k > 1 ? 16 : 0);
         rowT[er] = make_int4((kl * RS + jl) * mx, ((kl - 1) * JB + (jl - 1)) * mx, ys * (j + 1) + zs * (k + 1),
-                             ((j + k) & 1) | far);
+                             (j + k) & 1);
         rowC[4 * er + 0] = sc.cN[j];
         rowC[4 * er + 1] = sc.cS[j];
         rowC[4 * er + 2] = sc.cF[k];
@@ -579,13 +587,40 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     zero_published();
     if (!grid_sync(bar, nbar, nblocks, &s_flag)) failed = true;
 
+    // ---- the face ring of the other colour's tile from the neighbour bricks' rows,
+    // published before the last grid barrier: loads through L2 only (the rows change
+    // between half-sweeps, and this SM's L1 may hold an older copy), kFill per thread
+    // in flight, then the stores and a CTA barrier
+    const unsigned int mMX = 0xffffffffu / (unsigned)mx + 1u;   // q / mx, exact for q * mx < 2^32 (mx >= 3)
+    auto fill_ring = [&](int c) {
+        Tc* const O = c ? S0 : S1;
+        const Tc* const Og = c ? eRg : eBg;
+        const int tot = nring * mx;
+        for (int q0 = 0; q0 < tot; q0 += NT * kFill) {
+            Tc v[kFill];
+            int dst[kFill];
+#pragma unroll
+            for (int u = 0; u < kFill; ++u) {
+                const int q = min(q0 + tid + NT * u, tot - 1);
+                const unsigned int r = __umulhi((unsigned)q, mMX);
+                const int m = q - (int)r * mx;
+                const int2 rr = ringT[r];
+                dst[u] = rr.y >= 0 && q0 + tid + NT * u < tot ? rr.x + m : -1;
+                v[u] = __ldcg(Og + max(rr.y, 0) + m);
+            }
+#pragma unroll
+            for (int u = 0; u < kFill; ++u)
+                if (dst[u] >= 0) O[dst[u]] = v[u];
+        }
+        __syncthreads();
+    };
+
     // ---- one half-sweep of colour c over rows [e0r, e1r) (edge rows: EDGE)
     auto rows_pass = [&](auto edge_tag, int c, int e0r, int e1r, B& ch) {
         constexpr bool EDGE = decltype(edge_tag)::value;
         Tc* const W = c ? S1 : S0;
         const Tc* const O = c ? S0 : S1;
         Tc* const Ec = c ? eBg : eRg;
-        const Tc* const Og = c ? eRg : eBg;   // the other colour, as the neighbour bricks publish it
         const Tc* const Dg = c ? dBg : dRg;
         const Tc* const Rg = c ? rdBg : rdRg;
         const Tc* const Ds = c ? D1 : D0;
@@ -601,7 +636,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             w.cS = rowC[4 * er + 1];
             w.cF = rowC[4 * er + 2];
             w.cB = rowC[4 * er + 3];
-            w.far = rt.w;
+            w.par = rt.w;
             w.gr = rt.z;
             return w;
         };
@@ -612,14 +647,14 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             for (int er = e0r + 2 * warp; er < e1r; er += 2 * NWARP) {
                 const bool twoRows = er + 1 < e1r;
                 const ResRow<Tc> wA = row_of(er), wB = row_of(twoRows ? er + 1 : er);
-                const int rA = (wA.far ^ c) & 1, rB = (wB.far ^ c) & 1;
+                const int rA = (wA.par ^ c) & 1, rB = (wB.par ^ c) & 1;
                 const bool okA = lane < (rA ? nown1 : nown0);
                 const bool okB = twoRows && lane < (rB ? nown1 : nown0);
                 auto two = [&](auto ra, auto rb) {
                     constexpr int RA = decltype(ra)::value, RB = decltype(rb)::value;
                     const int mA = lane + 2 - RA, mB = lane + 2 - RB;
-                    const ResIn<Tc> xA = res_load<Tc, CD, CR, EDGE, RA>(wA, mA, mx, plane, Og, ys, zs);
-                    const ResIn<Tc> xB = res_load<Tc, CD, CR, EDGE, RB>(wB, mB, mx, plane, Og, ys, zs);
+                    const ResIn<Tc> xA = res_load<Tc, CD, CR, RA>(wA, mA, mx, plane);
+                    const ResIn<Tc> xB = res_load<Tc, CD, CR, RB>(wB, mB, mx, plane);
                     res_finish<Tc, EDGE>(xA, wA, mA, cEr[RA][0], cWr[RA][0], om, okA, Ec, ch);
                     res_finish<Tc, EDGE>(xB, wB, mB, cEr[RB][0], cWr[RB][0], om, okB, Ec, ch);
                 };
@@ -634,23 +669,23 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         } else {
             for (int er = e0r + warp; er < e1r; er += NWARP) {
                 const ResRow<Tc> w = row_of(er);
-                const int r = (w.far ^ c) & 1;
+                const int r = (w.par ^ c) & 1;
                 const int nown = r ? nown1 : nown0;
                 auto one = [&](auto rr) {
                     constexpr int R = decltype(rr)::value;
                     if constexpr (MODE == kResWide1) {
                         // cells t = lane (always in the row: it holds more than 32) and lane + 32
                         const int mA = lane + 2 - R;
-                        const ResIn<Tc> xA = res_load<Tc, CD, CR, EDGE, R>(w, mA, mx, plane, Og, ys, zs);
-                        const ResIn<Tc> xB = res_load<Tc, CD, CR, EDGE, R>(w, mA + 32, mx, plane, Og, ys, zs);
+                        const ResIn<Tc> xA = res_load<Tc, CD, CR, R>(w, mA, mx, plane);
+                        const ResIn<Tc> xB = res_load<Tc, CD, CR, R>(w, mA + 32, mx, plane);
                         res_finish<Tc, EDGE>(xA, w, mA, cEr[R][0], cWr[R][0], om, true, Ec, ch);
                         res_finish<Tc, EDGE>(xB, w, mA + 32, cEr[R][1], cWr[R][1], om, lane + 32 < nown, Ec, ch);
                     } else {
                         for (int t0 = 0; t0 < nown; t0 += 64) {
                             const int tA = t0 + lane;
                             const int mA = tA + 2 - R;
-                            const ResIn<Tc> xA = res_load<Tc, CD, CR, EDGE, R>(w, mA, mx, plane, Og, ys, zs);
-                            const ResIn<Tc> xB = res_load<Tc, CD, CR, EDGE, R>(w, mA + 32, mx, plane, Og, ys, zs);
+                            const ResIn<Tc> xA = res_load<Tc, CD, CR, R>(w, mA, mx, plane);
+                            const ResIn<Tc> xB = res_load<Tc, CD, CR, R>(w, mA + 32, mx, plane);
                             const int iA = min(2 * tA + 2 - R, g.nx + 2), iB = min(iA + 64, g.nx + 2);
                             const Tc eA = cEs[iA], wA = cWs[iA], eB = cEs[iB], wB = cWs[iB];
                             res_finish<Tc, EDGE>(xA, w, mA, eA, wA, om, tA < nown, Ec, ch);
@@ -673,7 +708,8 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         const int sg = done + s;   // sweep of this launch: ring slot
         if (blockIdx.x == 0 && tid == 0) ring[(sg + 1) % 3] = 0ULL;
         B ch = B(0);
-        // red half: the edge rows, arrive, the interior rows, wait
+        // red half: the ring, the edge rows, arrive, the interior rows, wait
+        fill_ring(0);
         rows_pass(EdgeT{}, 0, 0, ne, ch);
         grid_arrive(bar, nbar);
         rows_pass(InnerT{}, 0, ne, nrows, ch);
@@ -684,6 +720,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         // black half: the edge rows, the interior rows, then this CTA's max |change|
         // over the sweep into the ring slot of sweep sg and a full barrier, so that
         // every CTA's max is in the ring before anyone reads it
+        fill_ring(1);
         rows_pass(EdgeT{}, 1, 0, ne, ch);
         rows_pass(InnerT{}, 1, ne, nrows, ch);
 #pragma unroll
