@@ -75,6 +75,31 @@ __device__ __forceinline__ double defect_value(double cE, double pe, double cW, 
     return sub_rn(fma_rn(rd, s, -bv), pc);
 }
 
+// The FP64 defect of p + e from the defect d of p and the correction e of a
+// defect-correction cycle: since the operator is linear,
+//     d' = rdiag sum c (p+e)_nb - b' - (p+e) = d + rdiag sum_nb c_nb e_nb - e,
+// formed in FP64 with the FP64 coefficients from the cycle's (exact) Tc
+// values of e.  rdiag is the FP64 reciprocal of the coefficient sum, refined
+// from the sweeps' rd by two Newton steps.  Both SOR paths restart a cycle
+// with it.
+template <class Tc>
+__device__ __forceinline__ double defect_update(double cE, Tc eE, double cW, Tc eW, double cN, Tc eN, double cS,
+                                                Tc eS, double cF, Tc eF, double cB, Tc eB, Tc rd, Tc d, Tc e) {
+    double s = mul_rn(cE, (double)eE);
+    s = fma_rn(cW, (double)eW, s);
+    s = fma_rn(cN, (double)eN, s);
+    s = fma_rn(cS, (double)eS, s);
+    s = fma_rn(cF, (double)eF, s);
+    s = fma_rn(cB, (double)eB, s);
+    const double sum = ((cE + cW) + (cN + cS)) + (cF + cB);
+    double x = (double)rd;
+    double r = fma_rn(-sum, x, 1.0);
+    x = fma_rn(x, r, x);
+    r = fma_rn(-sum, x, 1.0);
+    x = fma_rn(x, r, x);
+    return sub_rn(fma_rn(x, s, (double)d), (double)e);
+}
+
 // Column-walking kernel (k_rhs): a 32 x 8 block covers (i, j) and
 // walks the planes of its chunk k0..k1 (chunk = blockIdx.z, chunks of
 // ceil(nz / gridDim.z) planes), carrying the k-1 value in a register, so a
@@ -118,17 +143,19 @@ __global__ void __launch_bounds__(kWalkBX * kWalkBY) k_rhs(Geom g, SorCoef<doubl
 }
 
 // Defect d = rdiag*sum c p0_nb - b' - p0 in double, stored per colour in
-// Tc; e reset to 0.  Inside the step graph (in_graph = 1) it also arms the
-// inner loop's condition.
+// Tc; e reset to 0.  With incr = 1, from the solve's second correction cycle
+// on (ctl->cycles > 0), d is instead updated from the last cycle's correction
+// (defect_update) and e is left for k_clear_e.  Inside the step graph
+// (in_graph = 1) it also arms the inner loop's condition.
 // For the resident path (ring != null) it also clears the ring of sweep
 // maxima and the grid barrier the next kernel uses, and with begin = 1 it
 // starts the solve (the counters k_sor_begin resets).
 template <class Tc>
 __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, const double* p,
                                                 const double* b, Tc* dR, Tc* dB, Tc* eR, Tc* eB,
-                                                Ctl* ctl, cudaGraphConditionalHandle inner,
-                                                int in_graph, unsigned long long* ring,
-                                                unsigned int* bar, int begin) {
+                                                const Tc* rdR, const Tc* rdB, Ctl* ctl,
+                                                cudaGraphConditionalHandle inner, int in_graph,
+                                                unsigned long long* ring, unsigned int* bar, int begin, int incr) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
@@ -150,13 +177,37 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
         if (bar) { bar[0] = 0u; bar[2] = 0u; }   // GridBar count and err
     }
     if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long q = spl(g, (i + 2) >> 1, j, k);
+    const bool red = ((i + j + k) & 1) == 0;
+    if (incr && ctl->cycles > 0) {
+        // the neighbours (other colour) at m(i-1) = (i+1)>>1, m(i+1) = (i+3)>>1, rows +-1
+        const Tc* O = red ? eB : eR;
+        const long long r0 = q - ((i + 2) >> 1);
+        const Tc dv = (red ? dR : dB)[q];
+        const double dn = defect_update(sc.cE[i], O[r0 + ((i + 3) >> 1)], sc.cW[i], O[r0 + ((i + 1) >> 1)], sc.cN[j],
+                                        O[q + g.mxp], sc.cS[j], O[q - g.mxp], sc.cF[k], O[q + g.mz], sc.cB[k],
+                                        O[q - g.mz], (red ? rdR : rdB)[q], dv, (red ? eR : eB)[q]);
+        (red ? dR : dB)[q] = (Tc)dn;
+        return;
+    }
     const long long c = nat(g, i, j, k);
     const double d = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], sc.cN[j], p[c + g.px], sc.cS[j],
                                   p[c - g.px], sc.cF[k], p[c + g.pz], sc.cB[k], p[c - g.pz], rdiag_of(sc, i, j, k),
                                   b[c], p[c]);
-    const long long q = spl(g, (i + 2) >> 1, j, k);
-    if (((i + j + k) & 1) == 0) { dR[q] = (Tc)d; eR[q] = Tc(0); }
+    if (red) { dR[q] = (Tc)d; eR[q] = Tc(0); }
     else { dB[q] = (Tc)d; eB[q] = Tc(0); }
+}
+
+// e = 0 on the interior cells of both colours (after an incremental defect).
+template <class Tc>
+__global__ void __launch_bounds__(256) k_clear_e(Geom g, Tc* eR, Tc* eB) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long q = spl(g, (i + 2) >> 1, j, k);
+    if (((i + j + k) & 1) == 0) eR[q] = Tc(0);
+    else eB[q] = Tc(0);
 }
 
 // rd = 1 / sum of the six coefficients of every interior cell, per colour,

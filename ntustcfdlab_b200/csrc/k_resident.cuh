@@ -5,22 +5,23 @@
 // The interior rows (j,k) are split into nbj x nbk bricks of at most JB x KB
 // rows; CTA b owns brick (b % nbj, b / nbj) and keeps e of both colours for
 // its rows in shared memory (colour-split rows of mx entries, see
-// ntcfd_common.cuh; the tile has a one-row ring that stays 0 and stands for
-// the domain's ghost rows), and the defect d and 1/diag rd of its rows when
-// they fit.  A half-sweep updates the CTA's cells of one colour, the
-// brick-boundary rows first: they read the neighbour bricks' rows straight
-// from the global e arrays (L2), where every CTA publishes its own boundary
-// rows as it updates them; then the CTA arrives at a grid barrier, updates
-// its interior rows from shared memory only and waits.  The sweep count,
-// the stop rule (GS.f90:11,53), the count of correction cycles and the final
-// p += e run inside the kernel, and so do the FP64 defect passes: the first
-// one at the start, and at every restart of the defect correction (a cycle
-// ending on its length, cycle_len sweeps): p += e, e = 0 (its published
-// boundary rows included), grid barrier, defect of the brick, sweeps on from
-// e = 0.  A defect pass stages p of the brick and its ring in shared memory
-// (over the e tile, which is free then) a slab of planes at a time and forms
-// d = rdiag sum c p_nb - b' - p from there (defect_value, the arithmetic of
-// k_defect); the staging is one bulk (TMA) copy per row of p and b'.
+// ntcfd_common.cuh) with a one-row ring, and the defect d and 1/diag rd of its
+// rows when they fit.  The ring rows of a domain boundary stay 0; the others
+// hold the neighbour bricks' boundary rows, which every CTA publishes to the
+// global e arrays as it updates them and copies into its ring ("fill") once
+// per half-sweep.  A sweep runs
+//     red:   [fill the black ring] -> interior rows -> edge rows -> arrive
+//     black: interior rows (own red values only) -> wait -> fill the red ring
+//            -> edge rows -> max |change| -> grid barrier,
+// so the fill latency overlaps the red interior rows and the first barrier
+// overlaps the black interior rows.  The sweep count, the stop rule
+// (GS.f90:11,53), the count of correction cycles and the final p += e run
+// inside the kernel, and so do the restarts of the defect correction: when a
+// cycle ends on its length (cycle_len sweeps), the kernel refreshes the black
+// ring, adds e to p and updates d to the FP64 defect of p + e
+// (defect_update: d + rdiag sum c e_nb - e, in FP64, from the exact FP32
+// values of e) without a grid barrier, then sweeps on from e = 0.  The first
+// defect of the solve comes from k_defect.
 //
 // A lane updates two cells at a time with every load issued before any
 // store: cells t and t + 32 of one row (rows of at most 64 cells per colour,
@@ -44,7 +45,7 @@
 namespace ntcfd {
 
 struct GridBar {
-    unsigned int count;   // arrivals since the launch began (k_resident_begin zeroes it)
+    unsigned int count;   // arrivals since the launch began (k_defect zeroes it)
     unsigned int gen;     // unused
     int err;
     int pad;
@@ -84,7 +85,9 @@ inline size_t resident_smem(const Brick& b, int nx) {
 }
 
 constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without sleep
-constexpr int kFill = 8;                            // loads in flight per thread when filling the ring
+// ring values a thread holds in flight while it updates interior rows (32 bytes)
+template <class Tc>
+constexpr int kFillOf = 32 / (int)sizeof(Tc);
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
     unsigned int v;
@@ -95,44 +98,6 @@ __device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v)
     asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
-
-// Bulk (TMA) copies of whole rows from global to shared memory, completed on
-// an mbarrier.  A copy starts on 16-byte boundaries at both ends and moves a
-// multiple of 16 bytes; no cluster multicast.
-__device__ __forceinline__ unsigned int smem_u32(const void* q) {
-    return (unsigned int)__cvta_generic_to_shared(q);
-}
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned int count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned int bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned int parity) {
-    unsigned int ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0u;
-}
-__device__ __forceinline__ void bulk_row_to_smem(void* dst, const void* src, unsigned int bytes,
-                                                 unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-// Orders this thread's generic-proxy accesses (shared memory, and global data
-// acquired from other CTAs) before the async-proxy copies it issues next.
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-}
 
 // Grid-wide barrier of one cooperative launch, split into arrive and wait so
 // that a CTA can work between the two.  One 32-bit word counts the arrivals
@@ -180,25 +145,6 @@ __device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int& nbar, unsign
                                           unsigned long long* dst = nullptr) {
     grid_arrive(b, nbar);
     return grid_wait(b, nbar, nblocks, s_flag, src, dst);
-}
-
-// Start of a resident solve: the counters of the control block, the ring of
-// sweep maxima and the grid barrier of the launch that follows.
-__global__ void k_resident_begin(Ctl* ctl, unsigned long long* ring, GridBar* bar) {
-    ctl->ik = 0;
-    ctl->inner = 0;
-    ctl->cycles = 0;
-    ctl->restarts = 0;
-    ctl->bodies = 0;
-    ctl->timeout = 0;
-    ctl->converged = 0;
-    ctl->nonfinite = 0;
-    ctl->last_change = 0.0;
-    ring[0] = 0ULL;
-    ring[1] = 0ULL;
-    ring[2] = 0ULL;
-    bar->count = 0u;
-    bar->err = 0;
 }
 
 // Row e of a brick's edge ring (jl or kl on the brick boundary), for e < ne,
@@ -284,9 +230,9 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
                unsigned long long* ring) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using B = decltype(abs_bits(Tc(0)));
+    constexpr int kFill = kFillOf<Tc>;
     __shared__ int s_flag;
     __shared__ unsigned long long s_ring;
-    __shared__ __align__(8) unsigned long long s_mbar;   // completion of the staging copies
     __shared__ B s_red[NT / 32];
     const int JB = br.JB, KB = br.KB, mx = br.mx;
     const int RS = JB + 2;                    // rows per k-plane of the tile
@@ -330,10 +276,6 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     // cells of a colour in a row of parity r
     const int nown0 = g.nx / 2, nown1 = (g.nx + 1) / 2;
 
-    if (tid == 0) {
-        mbar_init(&s_mbar, 1u);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
     for (int q = tid; q < 2 * tile; q += NT) S0[q] = Tc(0);
     for (int i = tid - 1; i <= g.nx + 2; i += NT) {
         cEs[i] = sc.cE[i];
@@ -379,15 +321,22 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         rowC[4 * er + 2] = sc.cF[k];
         rowC[4 * er + 3] = sc.cB[k];
     }
-    if (CR) {
-        // one warp per row, lanes along m
+    if (CD || CR) {
+        // d (the solve's first defect, from k_defect) and rd of the brick: one warp per
+        // row, lanes along m
         for (int row = warp; row < nrows; row += NWARP) {
             const int jl = row % nj, kl = row / nj;
             const long long gq0 = spl(g, 0, j0 + jl, k0 + kl);
             const int sq0 = (kl * JB + jl) * mx;
             for (int m = lane; m < mx; m += 32) {
-                R0[sq0 + m] = rdRg[gq0 + m];
-                R1[sq0 + m] = rdBg[gq0 + m];
+                if (CD) {
+                    D0[sq0 + m] = dRg[gq0 + m];
+                    D1[sq0 + m] = dBg[gq0 + m];
+                }
+                if (CR) {
+                    R0[sq0 + m] = rdRg[gq0 + m];
+                    R1[sq0 + m] = rdBg[gq0 + m];
+                }
             }
         }
     }
@@ -450,167 +399,93 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         }
     };
 
-    // FP64 defect of the brick into D0/D1 (or the global d arrays), with p of the
-    // brick and its one-row ring and b' of the brick staged in shared memory over
-    // the e tile, a slab of KS planes at a time: one bulk copy per row, issued by
-    // warp 0 and completed on the mbarrier.  A p row holds i = -1 .. RWp-2 (RWp
-    // even: a multiple of 16 bytes, starting 48 bytes into a 64-byte aligned global
-    // row), a b' row i = 1 .. RWb (RWb even, 64-byte aligned start).  Then a warp
-    // takes the slab's rows, lanes along i, with the lane's cE, cW in registers;
-    // every operand of a cell is in shared memory, and rdiag is formed as rdiag_of
-    // forms it.
-    const int RWp = (g.nx + 5) & ~1, RWb = (g.nx + 1) & ~1, RJ = nj + 2;
-    const size_t stage_bytes = 2 * (size_t)tile * sizeof(Tc);
-    const int ks_fit = (int)((stage_bytes - 2 * (size_t)RJ * RWp * sizeof(double)) /
-                             (((size_t)RJ * RWp + (size_t)nj * RWb) * sizeof(double)));
-    const int KS = min(ks_fit, nk);
-    unsigned int mphase = 0;
+    // Restart of a correction cycle: d of every cell of the brick becomes the FP64
+    // defect of p + e (defect_update), from the tiles (both rings current); one warp
+    // per row, lanes along i, the lane's cE, cW in registers.
     constexpr int DU = 4;   // cells per lane per row and i-chunk
-    auto defect_brick = [&]() {
-        double* const P = reinterpret_cast<double*>(smem_raw);
-        for (int ks0 = 0; ks0 < nk; ks0 += KS) {
-            const int kn = min(KS, nk - ks0);
-            const int nrow = RJ * (kn + 2), nbrow = nj * kn;
-            double* const Bs = P + (size_t)nrow * RWp;
-            // the tile was read and written through the generic proxy: order that
-            // before the copies overwrite it
-            fence_proxy_async();
-            __syncthreads();
-            if (warp == 0) {
-                if (lane == 0)
-                    mbar_arrive_expect_tx(&s_mbar, (unsigned)(((size_t)nrow * RWp + (size_t)nbrow * RWb) * sizeof(double)));
-                __syncwarp();
-                for (int row = lane; row < nrow + nbrow; row += 32) {
-                    if (row < nrow) {
-                        const int kk = row / RJ, jj = row - kk * RJ;
-                        bulk_row_to_smem(P + (size_t)row * RWp, p + nat(g, -1, j0 - 1 + jj, k0 + ks0 - 1 + kk),
-                                         (unsigned)(RWp * sizeof(double)), &s_mbar);
-                    } else {
-                        const int r = row - nrow, kq = r / nj, jl = r - kq * nj;
-                        bulk_row_to_smem(Bs + (size_t)r * RWb, b + nat(g, 1, j0 + jl, k0 + ks0 + kq),
-                                         (unsigned)(RWb * sizeof(double)), &s_mbar);
-                    }
-                }
+    auto update_defect = [&]() {
+        for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
+            double ce[DU], cw[DU];
+#pragma unroll
+            for (int u = 0; u < DU; ++u) {
+                const int i = min(ic + lane + 32 * u, g.nx);
+                ce[u] = g.cE[i];
+                cw[u] = g.cW[i];
             }
-            // bounded wait for the slab (the copies are issued above, so it ends)
-            unsigned int polls = 0;
-            while (!mbar_try_wait(&s_mbar, mphase)) {
-                if (++polls > kBarrierPolls) {
-                    if (tid == 0) atomicExch(&bar->err, 1);
-                    break;
-                }
-            }
-            mphase ^= 1u;
-            for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
-                double ce[DU], cw[DU];
+            for (int row = warp; row < nrows; row += NWARP) {
+                const int jl = row % nj + 1, kl = row / nj + 1;
+                const int j = j0 + jl - 1, k = k0 + kl - 1;
+                const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
+                const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
+                const long long g0 = spl(g, 0, j, k);
 #pragma unroll
                 for (int u = 0; u < DU; ++u) {
-                    const int i = min(ic + lane + 32 * u, g.nx);
-                    ce[u] = g.cE[i];
-                    cw[u] = g.cW[i];
-                }
-                for (int r = warp; r < nbrow; r += NWARP) {
-                    const int kq = r / nj, jl = r - kq * nj + 1;
-                    const int kl = ks0 + kq + 1;
-                    const int j = j0 + jl - 1, k = k0 + kl - 1;
-                    const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-                    const double sNS = cN + cS, sFB = cF + cB;
-                    const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
-                    const double* Pr = P + (size_t)((kq + 1) * RJ + jl) * RWp + 1;   // Pr[i]: p(i, j, k)
-                    const double* Br = Bs + (size_t)r * RWb - 1;                     // Br[i]: b'(i, j, k)
-#pragma unroll
-                    for (int u = 0; u < DU; ++u) {
-                        const int i = ic + lane + 32 * u;
-                        if (i > g.nx) continue;
-                        const double rd = rcp_rn(((ce[u] + cw[u]) + sNS) + sFB);
-                        const double dval =
-                            defect_value(ce[u], Pr[i + 1], cw[u], Pr[i - 1], cN, Pr[i + RWp], cS, Pr[i - RWp], cF,
-                                         Pr[i + RJ * RWp], cB, Pr[i - RJ * RWp], rd, Br[i], Pr[i]);
-                        const int m = (i + 2) >> 1;
-                        const bool red = ((i + j + k) & 1) == 0;
-                        if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
-                        else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
-                    }
+                    const int i = ic + lane + 32 * u;
+                    if (i > g.nx) continue;
+                    const bool red = ((i + j + k) & 1) == 0;
+                    const Tc* O = red ? S1 : S0;
+                    const Tc* Wt = red ? S0 : S1;
+                    const int m = (i + 2) >> 1;
+                    const Tc dv = CD ? (red ? D0 : D1)[dr + m] : (red ? dRg : dBg)[g0 + m];
+                    const Tc rv = CR ? (red ? R0 : R1)[dr + m] : (red ? rdRg : rdBg)[g0 + m];
+                    const double dn = defect_update(ce[u], O[sr + ((i + 3) >> 1)], cw[u], O[sr + ((i + 1) >> 1)], cN,
+                                                    O[sr + mx + m], cS, O[sr - mx + m], cF, O[sr + plane + m], cB,
+                                                    O[sr - plane + m], rv, dv, Wt[sr + m]);
+                    if (CD) (red ? D0 : D1)[dr + m] = (Tc)dn;
+                    else (red ? dRg : dBg)[g0 + m] = (Tc)dn;
                 }
             }
-            __syncthreads();
-        }
-    };
-    // The same defect with every operand read from global memory (for tiles too
-    // small to stage a slab): rows of this brick (and the frozen ghosts) through L1,
-    // this CTA wrote them; rows of the neighbour bricks, written by other SMs, from
-    // L2 only.
-    auto defect_direct = [&]() {
-        for (int row = warp; row < nrows; row += NWARP) {
-            const int jl = row % nj + 1, kl = row / nj + 1;
-            const int j = j0 + jl - 1, k = k0 + kl - 1;
-            const long long c0 = nat(g, 0, j, k);
-            const int dr = ((kl - 1) * JB + (jl - 1)) * mx;
-            const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-            const bool nL1 = jl < nj || j == g.ny, sL1 = jl > 1 || j == 1;
-            const bool fL1 = kl < nk || k == g.nz, bL1 = kl > 1 || k == 1;
-            for (int i = 1 + lane; i <= g.nx; i += 32) {
-                const long long c = c0 + i;
-                const double pn = nL1 ? __ldca(p + c + g.px) : __ldcg(p + c + g.px);
-                const double ps = sL1 ? __ldca(p + c - g.px) : __ldcg(p + c - g.px);
-                const double pf = fL1 ? __ldca(p + c + g.pz) : __ldcg(p + c + g.pz);
-                const double pb = bL1 ? __ldca(p + c - g.pz) : __ldcg(p + c - g.pz);
-                const double ce = g.cE[i], cw = g.cW[i];
-                const double rd = rcp_rn(((ce + cw) + (cN + cS)) + (cF + cB));
-                const double dval = defect_value(ce, __ldca(p + c + 1), cw, __ldca(p + c - 1), cN, pn, cS, ps, cF,
-                                                 pf, cB, pb, rd, __ldg(b + c), __ldca(p + c));
-                const int m = (i + 2) >> 1;
-                const bool red = ((i + j + k) & 1) == 0;
-                if (CD) (red ? D0 : D1)[dr + m] = (Tc)dval;
-                else (red ? dRg : dBg)[spl(g, m, j, k)] = (Tc)dval;
-            }
-        }
-        __syncthreads();
-    };
-    // the published boundary rows of e, both colours, to zero
-    auto zero_published = [&]() {
-        for (int q = tid; q < ne * mx; q += NT) {
-            const int er = q / mx, m = q - er * mx;
-            const int gr = rowT[er].z;
-            eRg[gr + m] = Tc(0);
-            eBg[gr + m] = Tc(0);
         }
     };
     auto zero_tile = [&]() {
         for (int q = tid; q < 2 * tile; q += NT) S0[q] = Tc(0);
     };
 
-    // ---- the first defect of the solve; the neighbours read the published rows as e = 0
-    if (KS >= 1) defect_brick();
-    else defect_direct();
-    zero_tile();
-    zero_published();
-    if (!grid_sync(bar, nbar, nblocks, &s_flag)) failed = true;
 
     // ---- the face ring of the other colour's tile from the neighbour bricks' rows,
     // published before the last grid barrier: loads through L2 only (the rows change
-    // between half-sweeps, and this SM's L1 may hold an older copy), kFill per thread
-    // in flight, then the stores and a CTA barrier
+    // between half-sweeps, and this SM's L1 may hold an older copy).  fill_issue puts
+    // the first kFill per thread in flight into registers; fill_commit stores them,
+    // moves any further ones and ends with a CTA barrier.  For the red half the ring
+    // is the black one (c = 0), for the black half the red one.
     const unsigned int mMX = 0xffffffffu / (unsigned)mx + 1u;   // q / mx, exact for q * mx < 2^32 (mx >= 3)
-    auto fill_ring = [&](int c) {
+    const int ring_tot = nring * mx;
+    auto fill_issue = [&](int c, Tc (&v)[kFill]) {
+        const Tc* const Og = c ? eRg : eBg;
+#pragma unroll
+        for (int u = 0; u < kFill; ++u) {
+            const int q = min(tid + NT * u, ring_tot - 1);
+            const unsigned int r = __umulhi((unsigned)q, mMX);
+            const int2 rr = ringT[r];
+            v[u] = __ldcg(Og + max(rr.y, 0) + (q - (int)r * mx));
+        }
+    };
+    auto fill_commit = [&](int c, const Tc (&v)[kFill]) {
         Tc* const O = c ? S0 : S1;
         const Tc* const Og = c ? eRg : eBg;
-        const int tot = nring * mx;
-        for (int q0 = 0; q0 < tot; q0 += NT * kFill) {
-            Tc v[kFill];
+#pragma unroll
+        for (int u = 0; u < kFill; ++u) {
+            const int q = tid + NT * u;
+            if (q >= ring_tot) continue;
+            const unsigned int r = __umulhi((unsigned)q, mMX);
+            const int2 rr = ringT[r];
+            if (rr.y >= 0) O[rr.x + (q - (int)r * mx)] = v[u];
+        }
+        for (int q0 = NT * kFill; q0 < ring_tot; q0 += NT * kFill) {
+            Tc w[kFill];
             int dst[kFill];
 #pragma unroll
             for (int u = 0; u < kFill; ++u) {
-                const int q = min(q0 + tid + NT * u, tot - 1);
+                const int q = min(q0 + tid + NT * u, ring_tot - 1);
                 const unsigned int r = __umulhi((unsigned)q, mMX);
                 const int m = q - (int)r * mx;
                 const int2 rr = ringT[r];
-                dst[u] = rr.y >= 0 && q0 + tid + NT * u < tot ? rr.x + m : -1;
-                v[u] = __ldcg(Og + max(rr.y, 0) + m);
+                dst[u] = rr.y >= 0 && q0 + tid + NT * u < ring_tot ? rr.x + m : -1;
+                w[u] = __ldcg(Og + max(rr.y, 0) + m);
             }
 #pragma unroll
             for (int u = 0; u < kFill; ++u)
-                if (dst[u] >= 0) O[dst[u]] = v[u];
+                if (dst[u] >= 0) O[dst[u]] = w[u];
         }
         __syncthreads();
     };
@@ -708,21 +583,26 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         const int sg = done + s;   // sweep of this launch: ring slot
         if (blockIdx.x == 0 && tid == 0) ring[(sg + 1) % 3] = 0ULL;
         B ch = B(0);
-        // red half: the ring, the edge rows, arrive, the interior rows, wait
-        fill_ring(0);
+        Tc fv[kFill];
+        // red half: the black ring in flight (it is 0 in a cycle's first sweep), the
+        // interior rows, the ring, the edge rows (published), arrive
+        if (s > 0) fill_issue(0, fv);
+        rows_pass(InnerT{}, 0, ne, nrows, ch);
+        if (s > 0) fill_commit(0, fv);
         rows_pass(EdgeT{}, 0, 0, ne, ch);
         grid_arrive(bar, nbar);
-        rows_pass(InnerT{}, 0, ne, nrows, ch);
+        // black half: the interior rows (they read only this brick's red values) while
+        // the barrier completes, wait, the red ring, the edge rows (published), then this
+        // CTA's max |change| over the sweep into the ring slot of sweep sg and a full
+        // barrier, so that every CTA's max is in the ring before anyone reads it
+        rows_pass(InnerT{}, 1, ne, nrows, ch);
         if (!grid_wait(bar, nbar, nblocks, &s_flag)) {
             failed = true;
             break;
         }
-        // black half: the edge rows, the interior rows, then this CTA's max |change|
-        // over the sweep into the ring slot of sweep sg and a full barrier, so that
-        // every CTA's max is in the ring before anyone reads it
-        fill_ring(1);
+        fill_issue(1, fv);
+        fill_commit(1, fv);
         rows_pass(EdgeT{}, 1, 0, ne, ch);
-        rows_pass(InnerT{}, 1, ne, nrows, ch);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const B t2 = __shfl_xor_sync(0xffffffffu, ch, o);
@@ -756,19 +636,19 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     done += done_c;
     // another cycle only when this one ended on its length
     if (failed || conv || nonfinite || done_c < cycle_len || ik0 + done >= itmax) break;
-    // restart: p += e, then the FP64 defect from the updated p, with e = 0
-    add_e_to_p();
-    __syncthreads();
-    // the published boundary rows too: the neighbour bricks read them as this brick's e
-    zero_published();
-    if (!grid_sync(bar, nbar, nblocks, &s_flag)) {
-        failed = true;
-        break;
+    // restart: the black ring again (the neighbours' final black rows; the red one is
+    // current), p += e, d = the FP64 defect of p + e, e = 0.  No grid barrier: the
+    // next cycle's first red half reads a zero black ring, and its black half reads
+    // red rows published after the next barrier.
+    {
+        Tc fv[kFill];
+        fill_issue(0, fv);
+        fill_commit(0, fv);
     }
-    if (KS >= 1) defect_brick();
-    else defect_direct();
+    add_e_to_p();
+    update_defect();
+    __syncthreads();
     zero_tile();
-    // the next half-sweep reads d only of this CTA's own cells
     __syncthreads();
     ++restarts;
   }

@@ -437,10 +437,12 @@ int build_graph(ntcfd_ctx* ctx) {
             return fail(ctx, NTCFD_EINVAL, "the resident SOR kernel does not fit this grid on this device");
     }
     if (ctx->resident) {
-        // the resident kernel runs the whole solve (every defect pass and correction
-        // cycle), so the solve is two plain nodes: the counter reset and the kernel
+        // the resident kernel runs the whole solve (every correction cycle), so the
+        // solve is two plain nodes: the defect (which also starts the solve) and the kernel
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
-        GK(add_kernel(&n, G, dep, k_resident_begin, dim3(1), dim3(1), ctx->ctl, ctx->ring, ctx->bar));
+        GK(add_kernel(&n, G, dep, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
+                      (const double*)ctx->b, dR, dB, eR, eB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
+                      (cudaGraphConditionalHandle)0, 0, ctx->ring, (unsigned int*)ctx->bar, 1, 0));
         dep = {n};
         GK(add_kernel_ex(&n, G, dep, resident_kernel<Tc>(ctx->brick), dim3(ctx->res_grid), dim3(kResNT),
                          ctx->res_smem, true, g, sor_coef<Tc>(ctx), ctx->brick, ctx->p, (const double*)ctx->b,
@@ -459,9 +461,13 @@ int build_graph(ntcfd_ctx* ctx) {
         std::vector<cudaGraphNode_t> od;
         cudaGraphNode_t m;
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+        // the defect of p (first cycle) or its update from the last cycle's e (later
+        // cycles, as the resident kernel restarts), then e = 0
         GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
-                      (const double*)ctx->b, dR, dB, eR, eB, ctx->ctl, hin, 1,
-                      (unsigned long long*)nullptr, (unsigned int*)nullptr, 0));
+                      (const double*)ctx->b, dR, dB, eR, eB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
+                      hin, 1, (unsigned long long*)nullptr, (unsigned int*)nullptr, 0, 1));
+        od = {m};
+        GK(add_kernel(&m, outer, od, k_clear_e<Tc>, g3, b3, g, eR, eB));
         od = {m};
         cudaGraph_t inner;
         GK(add_while(&m, outer, od, hin, &inner));
@@ -520,10 +526,10 @@ int build_graph(ntcfd_ctx* ctx) {
         dep = {n};
     }
     // kernels of a step: predictor, rhs, project, force (2), bc (3), step_end, + LES, + diagnostic;
-    // + sor_begin and 3 per cycle (streaming) or 2 per solve (resident)
+    // + sor_begin and 4 per cycle (streaming) or 2 per solve (resident)
     const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->resident ? 2 : 3, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
+                  P.diag_divergence, fixed, ctx->resident ? 2 : 4, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
     GK(cudaGraphInstantiate(&ctx->exec, G, 0));
     return 0;
 }
@@ -549,8 +555,9 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         return 0;
     };
     if (ctx->resident) {
-        // the counter reset and one launch that runs every defect pass and cycle
-        k_resident_begin<<<1, 1, 0, st>>>(ctx->ctl, ctx->ring, ctx->bar);
+        // one defect (starting the solve) and one launch that runs every cycle
+        k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, (const Tc*)ctx->rdR,
+                                        (const Tc*)ctx->rdB, ctx->ctl, 0, 0, ctx->ring, (unsigned int*)ctx->bar, 1, 0);
         void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&p, (void*)&b, (void*)&eR,
                         (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
                         (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&omega, (void*)&zeta,
@@ -566,8 +573,9 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
     const int big_guard = ctx->csweeps > 1 ? 1 : 0;
     while (more) {
         {
-            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0, nullptr,
-                                            nullptr, 0);
+            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, (const Tc*)ctx->rdR,
+                                            (const Tc*)ctx->rdB, ctx->ctl, 0, 0, nullptr, nullptr, 0, 1);
+            k_clear_e<Tc><<<g3, b3, 0, st>>>(g, eR, eB);
             const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
@@ -623,7 +631,7 @@ int run_step_eager(ntcfd_ctx* ctx) {
     k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
     const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
-    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed, ctx->resident ? 2 : 3,
+    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed, ctx->resident ? 2 : 4,
                                 ctx->resident ? 0 : 2 * ctx->csweeps + 1);
     CK(cudaGetLastError());
     return 0;
@@ -726,7 +734,8 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
     if ((rc = timed([&] {
              k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
-                                                      ctx->ctl, 0, 0, nullptr, nullptr, 0);
+                                                      (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl, 0, 0,
+                                                      nullptr, nullptr, 0, 0);
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
@@ -740,14 +749,17 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
          }, &out->sweep_ms, 2)))
         return rc;
     // the resident kernel: one launch of `nsw` sweeps (zeta = 0, one cycle) on a scratch
-    // copy of p, less a launch of no sweep (the kernel's set-up, first defect and p += e)
+    // copy of p, less a launch of no sweep (the defect before it, the kernel's set-up and
+    // p += e)
     if (ctx->resident) {
         const int nsw = 50;
         double* pscratch = ctx->us;   // rewritten by the predictor every step
         CK(cudaMemcpyAsync(pscratch, ctx->p, ctx->nat_elems * sizeof(double), cudaMemcpyDeviceToDevice,
                            ctx->stream));
         auto resident = [&](const int* sweeps) {
-            k_resident_begin<<<1, 1, 0, ctx->stream>>>(ctx->ctl, ctx->ring, ctx->bar);
+            k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, pscratch, ctx->b, dR, dB, eR, eB,
+                                                     (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl, 0, 0,
+                                                     ctx->ring, (unsigned int*)ctx->bar, 1, 0);
             void* args[] = {(void*)&g, (void*)&sc, (void*)&ctx->brick, (void*)&pscratch, (void*)&ctx->b,
                             (void*)&eR, (void*)&eB, (void*)&dR, (void*)&dB, (void*)&ctx->rdR, (void*)&ctx->rdB,
                             (void*)&ctx->ctl, (void*)&ctx->bar, (void*)&P.omega, (void*)&kZeroZeta,
