@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
         ctl->inner = 0;
         if (in_graph) cudaGraphSetConditional(inner, 1u);
         if (ring) { ring[0] = 0ULL; ring[1] = 0ULL; ring[2] = 0ULL; }
-        if (bar) { bar[0] = 0u; bar[2] = 0u; }   // GridBar count and err
+        if (bar) { bar[0] = 0u; bar[1] = 0u; bar[2] = 0u; }   // GridBar word and err
     }
     if (i > g.nx || j > g.ny || k > g.nz) return;
     const long long q = spl(g, (i + 2) >> 1, j, k);

@@ -45,8 +45,10 @@
 namespace ntcfd {
 
 struct GridBar {
-    unsigned int count;   // arrivals since the launch began (k_defect zeroes it)
-    unsigned int gen;     // unused
+    // low 32 bits: arrivals since the launch began; high 32 bits: the sum over the
+    // sweeps' closing barriers of the CTAs whose max |change| was above zeta, plus
+    // 2^20 per CTA whose max was not finite (k_defect zeroes the word)
+    unsigned long long word;
     int err;
     int pad;
 };
@@ -89,41 +91,43 @@ constexpr unsigned int kBarrierPolls = 20000000u;   // ~1-2 s of polling without
 template <class Tc>
 constexpr int kFillOf = 32 / (int)sizeof(Tc);
 
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-    unsigned int v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void red_add_release(unsigned int* p, unsigned int v) {
-    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void red_add_release(unsigned long long* p, unsigned long long v) {
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ int vload(const int* p) { return *(const volatile int*)p; }
 
 // Grid-wide barrier of one cooperative launch, split into arrive and wait so
-// that a CTA can work between the two.  One 32-bit word counts the arrivals
-// of the launch: each CTA adds 1 per barrier with a release reduction (after
-// a CTA barrier, so the CTA's earlier global writes are published) and does
-// not wait for the add to come back; the n-th barrier of the launch is passed
-// once the word reaches n * nblocks.  Waiting polls the word with acquire
-// loads, checks the shared error flag every 1024 polls and gives up after
-// kBarrierPolls polls, setting the flag so that every CTA leaves at its next
-// wait.  Returns false on failure.
-__device__ __forceinline__ void grid_arrive(GridBar* b, unsigned int& nbar) {
+// that a CTA can work between the two.  One 64-bit word counts the arrivals of
+// the launch in its low half: each CTA adds 1 per barrier with a release
+// reduction (after a CTA barrier, so the CTA's earlier global writes are
+// published) and does not wait for the add to come back; the n-th barrier of
+// the launch is passed once the low half reaches n * nblocks.  A CTA may add
+// flags to the high half with its arrival (flags << 32); they are summed over
+// the launch, and a waiter reads the sum as it sees the barrier pass.  Waiting
+// polls the word with acquire loads, checks the shared error flag every 1024
+// polls and gives up after kBarrierPolls polls, setting the flag so that every
+// CTA leaves at its next wait.  Returns false on failure.
+__device__ __forceinline__ void grid_arrive(GridBar* b, unsigned int& nbar, unsigned int flags = 0u) {
     __syncthreads();
-    if (threadIdx.x == 0) red_add_release(&b->count, 1u);
+    if (threadIdx.x == 0) red_add_release(&b->word, 1ull | ((unsigned long long)flags << 32));
     ++nbar;
 }
 
-// With src non-null, thread 0 also copies *src (read after the barrier) to *dst
-// before the closing CTA barrier, so every thread sees the same value.
+// With hi non-null, thread 0 also stores the high half of the word as it saw
+// the barrier pass to *hi before the closing CTA barrier, so every thread sees it.
 __device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int nbar, unsigned int nblocks, int* s_flag,
-                                          const unsigned long long* src = nullptr,
-                                          unsigned long long* dst = nullptr) {
+                                          unsigned int* hi = nullptr) {
     if (threadIdx.x == 0) {
         const unsigned int target = nbar * nblocks;
         int fail = 0;
         unsigned int polls = 0;
-        while ((int)(ld_acquire(&b->count) - target) < 0) {
+        unsigned long long w;
+        while ((int)((unsigned int)(w = ld_acquire(&b->word)) - target) < 0) {
             if ((++polls & 1023u) == 0u) {
                 if (vload(&b->err) != 0) { fail = 1; break; }
                 if (polls > kBarrierPolls) {
@@ -134,18 +138,19 @@ __device__ __forceinline__ bool grid_wait(GridBar* b, unsigned int nbar, unsigne
             }
         }
         *s_flag = fail;
-        if (src) *dst = *(const volatile unsigned long long*)src;
+        if (hi) *hi = (unsigned int)(w >> 32);
     }
     __syncthreads();
     return *s_flag == 0;
 }
 
 __device__ __forceinline__ bool grid_sync(GridBar* b, unsigned int& nbar, unsigned int nblocks, int* s_flag,
-                                          const unsigned long long* src = nullptr,
-                                          unsigned long long* dst = nullptr) {
-    grid_arrive(b, nbar);
-    return grid_wait(b, nbar, nblocks, s_flag, src, dst);
+                                          unsigned int flags = 0u, unsigned int* hi = nullptr) {
+    grid_arrive(b, nbar, flags);
+    return grid_wait(b, nbar, nblocks, s_flag, hi);
 }
+
+constexpr unsigned int kNanFlag = 1u << 20;   // high-half flag of a CTA whose max |change| was not finite
 
 // Row e of a brick's edge ring (jl or kl on the brick boundary), for e < ne,
 // or of its interior, for e >= ne; nj x nk rows, ni = interior rows.
@@ -232,7 +237,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     using B = decltype(abs_bits(Tc(0)));
     constexpr int kFill = kFillOf<Tc>;
     __shared__ int s_flag;
-    __shared__ unsigned long long s_ring;
+    __shared__ unsigned int s_hi;
     __shared__ B s_red[NT / 32];
     const int JB = br.JB, KB = br.KB, mx = br.mx;
     const int RS = JB + 2;                    // rows per k-plane of the tile
@@ -355,6 +360,8 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         }
 
     unsigned int nbar = 0;   // grid barriers of this launch passed so far
+    unsigned int hi_prev = 0u;   // high half of the barrier word at the last closing barrier
+    bool tested = false;         // a stop test ran in this launch
     const unsigned int nblocks = gridDim.x;
     const int ik0 = ctl->ik;
     const Tc om = (Tc)omega;
@@ -610,26 +617,33 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         }
         if (lane == 0) s_red[warp] = ch;
         __syncthreads();
-        if (tid < 32) {
-            B b2 = (tid < NWARP) ? s_red[tid] : B(0);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const B t2 = __shfl_xor_sync(0xffffffffu, b2, o);
-                b2 = t2 > b2 ? t2 : b2;
-            }
-            if (tid == 0 && b2 != B(0)) atomicMax(&ring[sg % 3], widen_bits(b2));
+        // the CTA's max: whether it is above zeta (or not finite) rides on this CTA's
+        // arrival at the closing barrier; the value itself goes to the ring slot of
+        // the sweep after the arrival, off the critical path (the solve's last one is
+        // read after a final barrier)
+        unsigned long long mybits = 0ull;
+        unsigned int flags = 0u;
+        if (tid == 0) {
+            B b2 = B(0);
+            for (int q = 0; q < NWARP; ++q) b2 = s_red[q] > b2 ? s_red[q] : b2;
+            mybits = widen_bits(b2);
+            flags = (mybits >= kInfBits ? kNanFlag : 0u) |
+                    ((__longlong_as_double((long long)mybits) > zeta || mybits >= kInfBits) ? 1u : 0u);
         }
-        if (!grid_sync(bar, nbar, nblocks, &s_flag, &ring[sg % 3], &s_ring)) {
+        grid_arrive(bar, nbar, flags);
+        if (tid == 0 && mybits != 0ull) atomicMax(&ring[sg % 3], mybits);
+        if (!grid_wait(bar, nbar, nblocks, &s_flag, &s_hi)) {
             failed = true;
             break;
         }
+        const unsigned int over = s_hi - hi_prev;   // CTAs above zeta, + kNanFlag per non-finite one
+        hi_prev = s_hi;
         done_c = s + 1;
         const int ik = ik0 + done + done_c;
         if (ik % check_every == 0 || ik >= itmax) {
-            const unsigned long long bits = s_ring;
-            last = __longlong_as_double((long long)bits);
-            nonfinite = bits >= kInfBits;
-            conv = !nonfinite && !(last > zeta);
+            nonfinite = over >= kNanFlag;
+            conv = over == 0u;
+            tested = true;
             if (conv || nonfinite) break;
         }
     }
@@ -653,6 +667,10 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     ++restarts;
   }
     add_e_to_p();
+    // the max |change| of the last (tested) sweep, whose slot every CTA has reached
+    // through the release of a later arrival
+    if (!failed && tested && done > 0 && grid_sync(bar, nbar, nblocks, &s_flag) && tid == 0)
+        last = __longlong_as_double((long long)*(const volatile unsigned long long*)&ring[(done - 1) % 3]);
     if (blockIdx.x == 0 && tid == 0) {
         ctl->ik = ik0 + done;
         ctl->inner = done_c;
