@@ -331,6 +331,10 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
         const Tc* __restrict__ dR = dOwn + rb;
         const Tc* __restrict__ rR = rdOwn + rb;
         const Tc cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
+        // FP32: rdiag formed here as rdiag_of forms it (the same bits as the rd array,
+        // one stream less); FP64: read
+        constexpr bool kFormRd = sizeof(Tc) == 4;
+        const Tc sNS = cN + cS, sFB = cF + cB;
         const Tc om = (Tc)omega;
         const int half = (g.nx + 1) / 2;
         for (int tA = lane; tA < half; tA += 64) {
@@ -346,7 +350,9 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
                      nBA = oB[mA];
             const Tc nEB = oC[mB + r], nWB = oC[mB - 1 + r], nNB = oN[mB], nSB = oS[mB], nFB = oF[mB],
                      nBB = oB[mB];
-            const Tc dA = dR[mA], dB_ = dR[mB], e0A = eR[mA], e0B = eR[mB], rdA = rR[mA], rdB = rR[mB];
+            const Tc dA = dR[mA], dB_ = dR[mB], e0A = eR[mA], e0B = eR[mB];
+            const Tc rdA = kFormRd ? rcp_rn(((eA + wA) + sNS) + sFB) : rR[mA];
+            const Tc rdB = kFormRd ? rcp_rn(((eB + wB) + sNS) + sFB) : rR[mB];
             Tc e1A, e1B;
             const Tc diffA = sor_update(eA, nEA, wA, nWA, cN, nNA, cS, nSA, cF, nFA, cB, nBA, rdA, dA, e0A, om, &e1A);
             const Tc diffB = sor_update(eB, nEB, wB, nWB, cN, nNB, cS, nSB, cF, nFB, cB, nBB, rdB, dB_, e0B, om, &e1B);

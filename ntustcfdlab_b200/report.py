@@ -3,13 +3,15 @@ plain FP64 path and of the mixed path, SOR sweeps per step, relative L2
 difference of the mixed state from the FP64 state after the same steps, and
 the largest |div u| V of the last step.
 
-    python -m ntustcfdlab_b200.report [--cases c1,c2,c3,c4,c5] [--out report.json]
+    python -m ntustcfdlab_b200.report [--cases c1,c2,c3,c4,c5] [--steps N] [--adjoint K] [--out f.json]
 
 Each case starts from its own initial state (zero fields, or the uniform
-inflow for the cylinder), builds its mask, runs a few untimed steps for the
-graph instantiation, resets, and times `steps` steps with the CUDA events of
-ntcfd_step.  The big airfoil cases run a fixed window of their first steps,
-stated in the output.
+inflow for the cylinder), builds its mask, runs two untimed steps for the
+graph instantiation, resets, and runs its configured number of steps (C1 200,
+C2 500, C3 1000, C4 200, C5 2000) timed with the CUDA events of ntcfd_step, in
+both precisions.  It reports the fraction of steps whose SOR solve converged
+before itmax, the divergence norm and, for C5 with --adjoint K, the adjoint of
+the mean lift coefficient over the last K steps.
 """
 from __future__ import annotations
 
@@ -22,9 +24,10 @@ from . import cases
 from .abi import FP64, MIXED, params_copy
 from .solver import Solver
 
-# case -> (factory, steps timed, mixed_cycle)
-WINDOWS = {"c1": (cases.c1, 200), "c2": (cases.c2, 500), "c3": (cases.c3, 50),
-           "c4": (cases.c4, 200), "c5": (cases.c5, 10)}
+# case -> (factory, steps of the configuration)
+WINDOWS = {"c1": (cases.c1, 200), "c2": (cases.c2, 500), "c3": (cases.c3, 1000),
+           "c4": (cases.c4, 200), "c5": (cases.c5, 2000)}
+CHUNK = 100   # steps per ntcfd_step call
 
 
 def _initial_state(case):
@@ -45,8 +48,25 @@ def _solver(case):
     return s
 
 
-def run_case(name: str, cycle: int = 8) -> dict:
-    fn, steps = WINDOWS[name]
+def _device_used_gb():
+    try:
+        import torch
+        free, total = torch.cuda.mem_get_info()
+        return (total - free) / 1e9
+    except Exception:
+        return None
+
+
+def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int = 0, M: int = 25,
+             log=print) -> dict:
+    """Both precisions over the case's steps from its initial state (after two
+    untimed steps for the graph instantiation and a reset).  With adjoint_K, the
+    mixed run saves its state K steps before the end and, after the run, the
+    discrete adjoint of the mean cLift over those K steps is taken from it
+    (checkpoints every M steps), with respect to the inflow direction of the
+    Back wall (normal w, tangential v) and its speed."""
+    fn, default_steps = WINDOWS[name]
+    steps = steps or default_steps
     out = {"case": name, "steps": steps}
     states = {}
     for prec, tag in ((FP64, "fp64"), (MIXED, "mixed")):
@@ -62,15 +82,47 @@ def run_case(name: str, cycle: int = 8) -> dict:
             s.step(2)                       # graph instantiation, outside the timed steps
             s.set_state(*st0)
             s.boundary_conditions()
-            info, rc = s.step(steps)
-            ms = s.last_step_ms()
+            info, ms, saved = [], 0.0, None
+            done = 0
+            while done < steps:
+                if adjoint_K and prec == MIXED and done == steps - adjoint_K:
+                    saved = s.get_state()
+                n = min(CHUNK, steps - done)
+                if adjoint_K and prec == MIXED and done < steps - adjoint_K:
+                    n = min(n, steps - adjoint_K - done)
+                inf, rc = s.step(n)
+                info += inf
+                ms += s.last_step_ms()
+                done += n
+                if done % 500 == 0 or done == steps:
+                    log(f"  {name} {tag}: {done}/{steps} steps, {ms / done:.3f} ms/step, "
+                        f"sweeps {inf[-1].sor_iters}, converged {inf[-1].converged}")
             states[tag] = s.get_state()
+            sw = np.array([i.sor_iters for i in info])
+            conv = np.array([i.converged for i in info])
             out[tag] = {"ms_per_step": ms / steps, "mcell_steps_per_s": c.cells * steps / (ms * 1e3),
-                        "sweeps_per_step": float(np.mean([i.sor_iters for i in info])),
-                        "all_converged": bool(all(i.converged for i in info)),
-                        "div_max_last": info[-1].div_max,
+                        "sweeps_per_step": float(sw.mean()),
+                        "sweeps_first10": float(sw[:10].mean()), "sweeps_last100": float(sw[-100:].mean()),
+                        "converged_fraction": float(conv.mean()),
+                        "first_converged_step": int(np.argmax(conv)) + 1 if conv.any() else None,
+                        "all_converged": bool(conv.all()),
+                        "div_max_last": info[-1].div_max, "div_max_max": float(max(i.div_max for i in info)),
                         "sor_path": {1: "streaming", 2: "resident"}.get(info[0].sor_path),
                         "cDrag_last": info[-1].cDrag, "cLift_last": info[-1].cLift}
+            if prec == MIXED:
+                kt = s.time_kernels(10)
+                out[tag]["kernel_ms"] = {k: round(v, 5) for k, v in kt.items()}
+            if saved is not None:
+                s.set_state(*saved)
+                r = s.adjoint(adjoint_K, M, w_drag=0.0, w_lift=1.0, inflow=("Back", 2, 1), force_grad=False)
+                out["adjoint"] = {"K": adjoint_K, "M": M, "objective": "mean cLift over the last K steps",
+                                  "J": r["J"], "dJ_dtheta_inflow": r["dJ_dtheta"], "dJ_dU": r["dJ_dU"],
+                                  "total_ms": r["total_ms"], "forward_ms": r["forward_ms"],
+                                  "recompute_ms": r["recompute_ms"], "solve_ms": r["solve_ms"],
+                                  "adjoint_over_forward": r["total_ms"] / r["forward_ms"],
+                                  "adj_sweeps": r["adj_sweeps"], "adj_unconverged": r["adj_unconverged"],
+                                  "device_used_gb_after": _device_used_gb()}
+                log(f"  {name} adjoint: {out['adjoint']}")
         finally:
             s.close()
     out["mixed_over_fp64"] = out["mixed"]["mcell_steps_per_s"] / out["fp64"]["mcell_steps_per_s"]
@@ -87,16 +139,20 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", default="c1,c2,c3,c4,c5")
     ap.add_argument("--cycle", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=None, help="override the configured step count")
+    ap.add_argument("--adjoint", type=int, default=0, help="C5: adjoint of mean cLift over the last K steps")
     ap.add_argument("--out", default=None)
     args = ap.parse_args()
     res = []
     for name in args.cases.split(","):
-        r = run_case(name.strip(), args.cycle)
+        name = name.strip()
+        r = run_case(name, args.cycle, args.steps, args.adjoint if name == "c5" else 0,
+                     log=lambda m: print(m, flush=True))
         print(json.dumps(r), flush=True)
         res.append(r)
-    if args.out:
-        with open(args.out, "w") as f:
-            json.dump(res, f, indent=1)
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(res, f, indent=1)
 
 
 if __name__ == "__main__":
