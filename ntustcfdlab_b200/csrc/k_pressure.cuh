@@ -294,8 +294,9 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
 }
 
 // One half-sweep over colour `colour` (0 = red, (i+j+k) even), row form (used
-// for FP32 e).  One warp per row (j,k), rows j-fastest so that the warps of a block share their j+-1
-// neighbour rows; the colour's cells of a row are contiguous in the
+// for FP32 e).  A warp takes a row (j,k) at a time, striding over the rows
+// (rows j-fastest, so that neighbouring warps share their j+-1 neighbour
+// rows); the colour's cells of a row are contiguous in the
 // colour-split arrays (m = t + 2 - r, r = ((j+k)^colour)&1, i = 2t + 2 - r),
 // so the row's base offsets are formed once and each lane updates two cells
 // per step (t and t + 32) with every load issued before its stores.  With
@@ -314,9 +315,10 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
     }
     using B = decltype(abs_bits(Tc(0)));
     const int lane = threadIdx.x & 31;
-    const int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+    const int nrow = g.ny * g.nz;
+    const int nwarp = (int)gridDim.x * (NT / 32);
     B ch = B(0);   // max |change| as an order-preserving pattern (NaN stays on top)
-    if (row < g.ny * g.nz) {
+    for (int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5); row < nrow; row += nwarp) {
         const int j = row % g.ny + 1, k = row / g.ny + 1;
         const int r = ((j + k) ^ colour) & 1;
         const int ys = g.mxp;
@@ -369,10 +371,15 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
     block_max_bits<NT>(ch, &slots[sub * kSpread + (blockIdx.x & (kSpread - 1))]);
 }
 
-// Launch shape of k_sweep_rows: NT threads, one warp per row.
-inline dim3 sweep_grid(const Geom& g, int nt) {
+// Launch shape of k_sweep_rows: NT threads, warps striding over the rows, at
+// most kSweepRowBlocks blocks per SM (about the resident count), so a block's
+// max reduction and start-up are paid once for many rows.
+constexpr int kSweepRowBlocks = 6;
+inline dim3 sweep_grid(const Geom& g, int nt, int sms) {
     const long long rows = (long long)g.ny * g.nz;
-    return dim3((unsigned)((rows + nt / 32 - 1) / (nt / 32)));
+    const long long need = (rows + nt / 32 - 1) / (nt / 32);
+    const long long cap = (long long)kSweepRowBlocks * (sms > 0 ? sms : 1);
+    return dim3((unsigned)(need < cap ? need : cap));
 }
 
 // One warp: the max over the kSpread slots of that sweep is its max|change|.

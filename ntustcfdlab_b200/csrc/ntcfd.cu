@@ -55,7 +55,7 @@ template <>
 struct Sweep<double> {
     static constexpr auto fn = k_sweep_cols<double, kSweepBx * kSweepBy, kSweepKpt>;
     static dim3 block() { return dim3(kSweepBx, kSweepBy, 1); }
-    static dim3 grid(const Geom& g) {
+    static dim3 grid(const Geom& g, int) {
         const int half = (g.nx + 1) / 2;
         return dim3((half + kSweepBx - 1) / kSweepBx, (g.ny + kSweepBy - 1) / kSweepBy,
                     (g.nz + kSweepKpt - 1) / kSweepKpt);
@@ -65,7 +65,7 @@ template <>
 struct Sweep<float> {
     static constexpr auto fn = k_sweep_rows<float, kSweepNT>;
     static dim3 block() { return dim3(kSweepNT); }
-    static dim3 grid(const Geom& g) { return sweep_grid(g, kSweepNT); }
+    static dim3 grid(const Geom& g, int sms) { return sweep_grid(g, kSweepNT, sms); }
 };
 
 struct DevTabs {
@@ -476,7 +476,7 @@ int build_graph(ntcfd_ctx* ctx) {
             std::vector<cudaGraphNode_t> id;
             cudaGraphNode_t s;
             const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
             const Ctl* cctl = ctx->ctl;
             for (int sub = 0; sub < ctx->csweeps; ++sub) {
                 GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
@@ -576,7 +576,7 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
             k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, (const Tc*)ctx->rdR,
                                             (const Tc*)ctx->rdB, ctx->ctl, 0, 0, nullptr, nullptr, 0, 1);
             k_clear_e<Tc><<<g3, b3, 0, st>>>(g, eR, eB);
-            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
                     Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
@@ -739,7 +739,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-    const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g);
+    const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
     const int big = 1 << 30;
     if ((rc = timed([&] {
              Sweep<Tc>::fn<<<gs, bs, 0, ctx->stream>>>(

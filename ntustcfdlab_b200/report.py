@@ -114,13 +114,15 @@ def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int
                 out[tag]["kernel_ms"] = {k: round(v, 5) for k, v in kt.items()}
             if saved is not None:
                 s.set_state(*saved)
-                r = s.adjoint(adjoint_K, M, w_drag=0.0, w_lift=1.0, inflow=("Back", 2, 1), force_grad=False)
+                r = s.adjoint(adjoint_K, M, w_drag=0.0, w_lift=1.0, inflow=("Back", 2, 1), force_grad=False,
+                              adj_itmax=3000)
                 out["adjoint"] = {"K": adjoint_K, "M": M, "objective": "mean cLift over the last K steps",
                                   "J": r["J"], "dJ_dtheta_inflow": r["dJ_dtheta"], "dJ_dU": r["dJ_dU"],
                                   "total_ms": r["total_ms"], "forward_ms": r["forward_ms"],
                                   "recompute_ms": r["recompute_ms"], "solve_ms": r["solve_ms"],
                                   "adjoint_over_forward": r["total_ms"] / r["forward_ms"],
                                   "adj_sweeps": r["adj_sweeps"], "adj_unconverged": r["adj_unconverged"],
+                                  "adj_itmax": 3000,
                                   "device_used_gb_after": _device_used_gb()}
                 log(f"  {name} adjoint: {out['adjoint']}")
         finally:
