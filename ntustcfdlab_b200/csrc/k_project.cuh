@@ -429,9 +429,18 @@ __global__ void __launch_bounds__(NT) k_divmax(Geom g, const double* u, const do
 // Records the step; `fixed` kernels per step, per_cycle per correction cycle
 // (cycles restarted inside the resident SOR kernel launch nothing) and
 // per_body per inner loop body.
+// With forces = 0 (ETA is 0 everywhere, the force kernels did not run) it also
+// records the coefficients those kernels give for zero forces: -2 * 0 / lx.
 __global__ void k_step_end(Ctl* ctl, StepRec* rec, unsigned long long* divslot, int diag,
-                           int fixed, int per_cycle, int per_body) {
+                           int fixed, int per_cycle, int per_body, int forces, double lx) {
     const int s = ctl->step;
+    if (!forces) {
+        const double z = (-2.0) * 0.0 / lx;
+        ctl->cdrag = z;
+        ctl->clift = z;
+        rec[s].cdrag = z;
+        rec[s].clift = z;
+    }
     rec[s].launches = fixed + per_cycle * (ctl->cycles - ctl->restarts) + ctl->bodies * per_body;
     rec[s].timeout = ctl->timeout;
     rec[s].sor_iters = ctl->ik;

@@ -121,6 +121,7 @@ struct ntcfd_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_ms = 0.0f;
     bool metrics_set = false, coords_set = false;
+    bool mask_nonzero = false;              // ETA may be nonzero: the force kernels run
     double time = 0.0;
     int nchunk = 0, csweeps = 1, cycle_len = 1;
     std::vector<void*> allocs;
@@ -502,12 +503,15 @@ int build_graph(ntcfd_ctx* ctx) {
     GK(add_kernel(&n, G, dep, k_project, dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk),
                   dim3(32, 4, 1), g, pj));
     dep = {n};
-    GK(add_kernel(&n, G, dep, k_force_columns, dim3(296), dim3(256), g, (const double*)ctx->partZ,
-                  (const double*)ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz));
-    dep = {n};
-    GK(add_kernel(&n, G, dep, k_force_total<256>, dim3((g.nx + 7) / 8), dim3(256), g, (const double*)ctx->FXz,
-                  (const double*)ctx->FYz, ctx->FXy, ctx->FYy, P.lx, ctx->ctl, ctx->fdone, ctx->rec));
-    dep = {n};
+    // the force integral only where a mask can make forces (ETA = 0: zero by construction)
+    if (ctx->mask_nonzero) {
+        GK(add_kernel(&n, G, dep, k_force_columns, dim3(296), dim3(256), g, (const double*)ctx->partZ,
+                      (const double*)ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz));
+        dep = {n};
+        GK(add_kernel(&n, G, dep, k_force_total<256>, dim3((g.nx + 7) / 8), dim3(256), g, (const double*)ctx->FXz,
+                      (const double*)ctx->FYz, ctx->FXy, ctx->FYy, P.lx, ctx->ctl, ctx->fdone, ctx->rec));
+        dep = {n};
+    }
     BcArgs ba{};
     ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
     std::memcpy(ba.bc, P.bc, sizeof ba.bc);
@@ -525,11 +529,13 @@ int build_graph(ntcfd_ctx* ctx) {
                       (const double*)ctx->v, (const double*)ctx->w, ctx->divslot));
         dep = {n};
     }
-    // kernels of a step: predictor, rhs, project, force (2), bc (3), step_end, + LES, + diagnostic;
-    // + sor_begin and 4 per cycle (streaming) or 2 per solve (resident)
-    const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
+    // kernels of a step: predictor, rhs, project, force (2, with a mask), bc (3), step_end, + LES,
+    // + diagnostic; + sor_begin and 4 per cycle (streaming) or 2 per solve (resident)
+    const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
+                      (ctx->resident ? 0 : 1);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->resident ? 2 : 4, ctx->resident ? 0 : 2 * ctx->csweeps + 1));
+                  P.diag_divergence, fixed, ctx->resident ? 2 : 4, ctx->resident ? 0 : 2 * ctx->csweeps + 1,
+                  ctx->mask_nonzero ? 1 : 0, P.lx));
     GK(cudaGraphInstantiate(&ctx->exec, G, 0));
     return 0;
 }
@@ -617,9 +623,11 @@ int run_step_eager(ntcfd_ctx* ctx) {
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
     k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0, st>>>(g, pj);
-    k_force_columns<<<296, 256, 0, st>>>(g, ctx->partZ, ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz);
-    k_force_total<256><<<(g.nx + 7) / 8, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, P.lx,
-                                                          ctx->ctl, ctx->fdone, ctx->rec);
+    if (ctx->mask_nonzero) {
+        k_force_columns<<<296, 256, 0, st>>>(g, ctx->partZ, ctx->partY, ctx->nchunk, ctx->FXz, ctx->FYz);
+        k_force_total<256><<<(g.nx + 7) / 8, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, P.lx,
+                                                              ctx->ctl, ctx->fdone, ctx->rec);
+    }
     BcArgs ba{};
     ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
     std::memcpy(ba.bc, P.bc, sizeof ba.bc);
@@ -630,9 +638,10 @@ int run_step_eager(ntcfd_ctx* ctx) {
     k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
-    const int fixed = 9 + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) + (ctx->resident ? 0 : 1);
+    const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
+                      (ctx->resident ? 0 : 1);
     k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed, ctx->resident ? 2 : 4,
-                                ctx->resident ? 0 : 2 * ctx->csweeps + 1);
+                                ctx->resident ? 0 : 2 * ctx->csweeps + 1, ctx->mask_nonzero ? 1 : 0, P.lx);
     CK(cudaGetLastError());
     return 0;
 }
@@ -1034,6 +1043,25 @@ int ntcfd_set_coords(ntcfd_ctx* ctx, const double* X, const double* Y, const dou
     return 0;
 }
 
+// Whether ETA may be nonzero (the force kernels run).  A change rebuilds the
+// step graph; going to zero also clears the force-integral arrays, which the
+// adjoint reads as the step's guard pattern.
+static int set_mask_flag(ntcfd_ctx* ctx, bool nonzero) {
+    if (nonzero == ctx->mask_nonzero) return 0;
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
+    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    if (!nonzero) {
+        const size_t cols = (size_t)ctx->g.nx * ctx->g.ny;
+        CK(cudaMemsetAsync(ctx->FXz, 0, cols * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(ctx->FYz, 0, cols * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(ctx->FXy, 0, ctx->g.nx * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(ctx->FYy, 0, ctx->g.nx * sizeof(double), ctx->stream));
+    }
+    ctx->mask_nonzero = nonzero;
+    return 0;
+}
+
 static int copy_halo(ntcfd_ctx* ctx, double* dev, const double* host, bool to_dev) {
     const Geom& g = ctx->g;
     double* d0 = dev + nat(g, -1, -1, -1);
@@ -1053,7 +1081,10 @@ int ntcfd_set_mask(ntcfd_ctx* ctx, const double* eta) {
     int rc = copy_halo(ctx, ctx->eta, eta, true);
     if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
-    return 0;
+    const size_t n = (size_t)(ctx->g.nx + 4) * (ctx->g.ny + 4) * (ctx->g.nz + 4);
+    bool nz = false;
+    for (size_t q = 0; q < n && !nz; ++q) nz = eta[q] != 0.0;
+    return set_mask_flag(ctx, nz);
 }
 
 int ntcfd_get_mask(ntcfd_ctx* ctx, double* eta) {
@@ -1357,6 +1388,7 @@ int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
 int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r) {
     DEV();
     if (!ctx->metrics_set || !ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "metrics and coordinates first");
+    if (int rc = set_mask_flag(ctx, true)) return rc;
     const Geom& g = ctx->g;
     double* eta1 = ctx->outbuf;  // scratch: nz*ny
     k_cylinder<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
@@ -1374,6 +1406,7 @@ int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* 
     DEV();
     if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
     if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    if (int rc = set_mask_flag(ctx, true)) return rc;
     const Geom& g = ctx->g;
     // airfoil.f90:597-611 on the host: shift by the quarter chord, rotate by
     // -AOA (ay uses the already rotated az, as in the reference), translate.
@@ -1501,6 +1534,7 @@ extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az
     if (cells > (size_t)kNaCells)
         return fail(ctx, NTCFD_EINVAL, "ny*nz = %zu cells; the allocation-free variant takes at most %d",
                     cells, kNaCells);
+    if (int rc = set_mask_flag(ctx, true)) return rc;
     unsigned char* base = nullptr;
     if (int rc = noalloc_scratch(ctx, &base)) return rc;
     double* daz = reinterpret_cast<double*>(base);

@@ -353,3 +353,29 @@ def test_eager_launch_matches_graph(path):
     assert out[0][1] == out[1][1]
     for a, b in zip(out[0][0], out[1][0]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_force_kernels_run_only_with_a_mask():
+    """ETA = 0 everywhere makes the forces exactly zero, so the two force
+    kernels are left out of the step (two launches fewer) and the coefficients
+    are recorded as the kernels would give them; a nonzero mask brings them
+    back, and clearing it leaves them out again."""
+    from ntustcfdlab_b200 import cases
+    c = cases.cavity(24, 400.0, 1e-3, 2)
+    s = _solver(c.params, c.grid)
+    try:
+        s.boundary_conditions()
+        info0, _ = s.step(2)
+        assert all(i.cDrag == 0.0 and i.cLift == 0.0 for i in info0)
+        eta = np.zeros(s.halo_shape, order="F")
+        eta[10:16, 8:14, 9:13] = 1.0
+        s.set_mask(eta)
+        info1, _ = s.step(2)
+        assert all(b.launches == a.launches + 2 for a, b in zip(info0, info1))
+        assert any(i.cDrag != 0.0 for i in info1)
+        s.set_mask(np.zeros(s.halo_shape, order="F"))
+        info2, _ = s.step(2)
+        assert all(i.launches == info0[0].launches for i in info2)
+        assert all(i.cDrag == 0.0 and i.cLift == 0.0 for i in info2)
+    finally:
+        s.close()
