@@ -218,19 +218,20 @@ int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
  * with time the simulated time before the step and pi the reference's
  * default-real literal 3.14159265359, and rebuilds ETA by ray casting the
  * polygon (az, ay) at that angle about (zc, yc) as ntcfd_build_mask_polygon
- * does, through the allocation-free variant (so the limits of
- * ntcfd_build_mask_polygon_noalloc apply, checked here).  The angle used is
- * reported in ntcfd_step_info.aoa.  A step whose polygon meets an exact
- * vertex/grid tie stops the call with NTCFD_EINVAL (the reference moves the
- * grid instead); the steps before it have run, and per_step, ntcfd_time and
- * the step count account for exactly those.  npts = 0 switches the dynamic
- * angle off.
- *
- * The rebuild uses the allocation-free variant's device array, which every
- * context on a device shares: two contexts with a dynamic angle of attack on
- * one device whose ntcfd_step calls overlap (two host threads) race on it and
- * may build each other's masks.  Run such contexts one after the other, or
- * on different devices. */
+ * does.  The host evaluates each step's angle and its cosine and sine; the
+ * rotation, the ray casting and ETA are computed on the device inside the
+ * step's CUDA graph (a second graph: the mask kernels, then the step under a
+ * conditional node), so a call of many steps makes no per-step host round
+ * trip.  The arrays are the context's own (allocated here; no limit on npts
+ * or ny*nz beyond device memory), so contexts on one device do not share
+ * them.  The angle used is reported in ntcfd_step_info.aoa.  A step whose
+ * polygon meets an exact vertex/grid tie stops the call with NTCFD_EINVAL
+ * (the reference moves the grid instead): that step and the rest of the call
+ * do nothing, ETA holds the tied step's mask, and per_step, ntcfd_time and
+ * the step count account for exactly the steps that ran.  npts = 0 switches
+ * the dynamic angle off.  An eager context (or a driver that does not take
+ * the conditional graph) launches the same kernels one by one and reads the
+ * tie count after each step's mask. */
 int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
                           double aoa1, double reduce_frequency, double zc, double yc,
                           int start_step);

@@ -13,13 +13,11 @@
 
 namespace ntcfd {
 
-// ETA_1 from the crossing parity (airfoil.f90:685-764).
+// ETA_1 from the crossing parity (airfoil.f90:685-764) of cell (k,j).
 // Y, Z: node coordinates pre-offset (Y[j] valid for j in -1..n+3).
-__global__ void k_ray_main(int ny, int nz, const double* Y, const double* Z, const double* az,
-                           const double* ay, int poly, double* eta1, int* ties) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    if (k > nz || j > ny) return;
+__device__ __forceinline__ void ray_main_cell(int k, int j, int nz, const double* Y, const double* Z,
+                                              const double* az, const double* ay, int poly, double* eta1,
+                                              int* ties) {
     const double Yj = Y[j], Zk = Z[k];
     const double ycell = (Y[j] + Y[j + 1]) / 2.0;
     const double zcell = (Z[k] + Z[k + 1]) / 2.0;
@@ -53,12 +51,19 @@ __global__ void k_ray_main(int ny, int nz, const double* Y, const double* Z, con
     if (tie) atomicAdd(ties, tie);
 }
 
+__global__ void k_ray_main(int ny, int nz, const double* Y, const double* Z, const double* az,
+                           const double* ay, int poly, double* eta1, int* ties) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (k > nz || j > ny) return;
+    ray_main_cell(k, j, nz, Y, Z, az, ay, poly, eta1, ties);
+}
+
 // points(k,j) = 1 when a polygon vertex lies in [Z(k),Z(k+1)) x [Y(j),Y(j+1))
 // for k in C..E-1, j in A..B-1 (airfoil.f90:661-674).
-__global__ void k_ray_points(int ny, int nz, const double* Y, const double* Z, const double* az,
-                             const double* ay, int poly, int A, int B, int C, int E, int* points) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= poly) return;
+__device__ __forceinline__ void ray_point(int m, int ny, int nz, const double* Y, const double* Z,
+                                          const double* az, const double* ay, int A, int B, int C, int E,
+                                          int* points) {
     for (int k = C; k <= E - 1; ++k) {
         if (!(az[m] >= Z[k] && az[m] < Z[k + 1])) continue;
         for (int j = A; j <= B - 1; ++j)
@@ -67,14 +72,19 @@ __global__ void k_ray_points(int ny, int nz, const double* Y, const double* Z, c
     }
 }
 
-// Sub-grid volume fraction of cut cells (airfoil.f90:773-884): one block per
-// listed cell, one thread per group of sub-cells, ETA_1 = odd sub-cells / 2500.
+__global__ void k_ray_points(int ny, int nz, const double* Y, const double* Z, const double* az,
+                             const double* ay, int poly, int A, int B, int C, int E, int* points) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= poly) return;
+    ray_point(m, ny, nz, Y, Z, az, ay, A, B, C, E, points);
+}
+
+// Sub-grid volume fraction of cut cell `cell` (airfoil.f90:773-884): the
+// block's threads share the 50 x 50 sub-cells, ETA_1 = odd sub-cells / 2500.
 constexpr int kSub = 50;
 template <int NT>
-__global__ void __launch_bounds__(NT) k_ray_sub(int nz, const double* Y, const double* Z,
-                                                const double* az, const double* ay, int poly,
-                                                const int* cells, double* eta1, int* ties) {
-    const int cell = cells[blockIdx.x];
+__device__ __forceinline__ void ray_sub_cell(int cell, int nz, const double* Y, const double* Z, const double* az,
+                                             const double* ay, int poly, double* eta1, int* ties, int* red) {
     const int k = cell % nz + 1, j = cell / nz + 1;
     const double Yj = Y[j], Yj1 = Y[j + 1], Zk = Z[k], Zk1 = Z[k + 1];
     int odd = 0, tie = 0;
@@ -114,7 +124,6 @@ __global__ void __launch_bounds__(NT) k_ray_sub(int nz, const double* Y, const d
         }
         odd += (cnt % 2 != 0) ? 1 : 0;
     }
-    __shared__ int red[NT];
     red[threadIdx.x] = odd;
     __syncthreads();
     for (int s = NT / 2; s > 0; s >>= 1) {
@@ -125,7 +134,17 @@ __global__ void __launch_bounds__(NT) k_ray_sub(int nz, const double* Y, const d
         const double total = (double)red[0];
         eta1[(long long)(k - 1) + (long long)nz * (j - 1)] = total / (double)kSub / (double)kSub;
     }
+    __syncthreads();   // red is reused by the block's next cell
     if (tie) atomicAdd(ties, tie);
+}
+
+// One block per listed cell.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_ray_sub(int nz, const double* Y, const double* Z,
+                                                const double* az, const double* ay, int poly,
+                                                const int* cells, double* eta1, int* ties) {
+    __shared__ int red[NT];
+    ray_sub_cell<NT>(cells[blockIdx.x], nz, Y, Z, az, ay, poly, eta1, ties, red);
 }
 
 // ETA(i,j,k) = ETA_1(k,j) on the interior (airfoil.f90:889-891); ghosts 0.
@@ -136,6 +155,147 @@ __global__ void k_extrude(Geom g, const double* eta1, double* eta) {
     if (i > g.nx + 2 || j > g.ny + 2 || k > g.nz + 2) return;
     const bool in = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
     eta[nat(g, i, j, k)] = in ? eta1[(long long)(k - 1) + (long long)g.nz * (j - 1)] : 0.0;
+}
+
+// ---- The mask of a moving body on the device, one step at a time inside the
+// step graph (ntcfd_set_dynamic_aoa).  The host evaluates each step's angle
+// (airfoil.f90:313-317) and its cosine and sine; k_dyn_rotate turns the body
+// polygon by them (airfoil.f90:597-611) for the step the control block's step
+// counter names.  After a step whose polygon meets an exact vertex/grid tie (the
+// reference moves the grid instead) the control block's halt flag is set: the
+// mask kernels and, through the graph's IF node, the step itself do nothing
+// for the rest of the call.
+struct DynMask {
+    const double* base;   // body polygon: az[npts], then ay[npts]
+    const double* trig;   // cos, sin of each step of the call
+    double* poly;         // this step's polygon: az, then ay
+    int npts;
+    double zc, yc;
+    int* flags;           // ny*nz: cells that hold a vertex (k fastest)
+    int* list;            // ny*nz: those cells, compacted
+    int* meta;            // A, B, C, E (airfoil.f90:615-654), listed cells, ties
+    double* eta1;         // ETA_1(k,j)
+};
+
+// The step's polygon and its bounds A, B, C, E (airfoil.f90:615-654: A = the
+// first j with Y(j) > min ay, less one, 0 when there is none; B = the first j
+// with Y(j) > max ay; C, E likewise in z); the counters cleared.  One block.
+// The rotation keeps the reference's order of operations (the new az enters
+// the new ay) with every product and sum rounded on its own, as on the host.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_dyn_rotate(int ny, int nz, const double* Y, const double* Z, DynMask m,
+                                                   const Ctl* ctl) {
+    if (ctl->halt) return;
+    __shared__ double sd[4][NT];
+    __shared__ int si[4][NT];
+    const double c = m.trig[2 * ctl->step], sn = m.trig[2 * ctl->step + 1];
+    const int t = threadIdx.x;
+    double mny = INFINITY, mxy = -INFINITY, mnz = INFINITY, mxz = -INFINITY;
+    for (int q = t; q < m.npts; q += NT) {
+        const double z0 = __dsub_rn(m.base[q], 0.25), y0 = m.base[m.npts + q];
+        const double z1 = __dsub_rn(__dmul_rn(c, z0), __dmul_rn(sn, y0));
+        const double y1 = __dadd_rn(__dmul_rn(sn, z1), __dmul_rn(c, y0));
+        const double az = __dadd_rn(__dadd_rn(z1, m.zc), 0.25), ay = __dadd_rn(y1, m.yc);
+        m.poly[q] = az;
+        m.poly[m.npts + q] = ay;
+        mny = fmin(mny, ay); mxy = fmax(mxy, ay);
+        mnz = fmin(mnz, az); mxz = fmax(mxz, az);
+    }
+    sd[0][t] = mny; sd[1][t] = mxy; sd[2][t] = mnz; sd[3][t] = mxz;
+    __syncthreads();
+    for (int s = NT / 2; s > 0; s >>= 1) {
+        if (t < s) {
+            sd[0][t] = fmin(sd[0][t], sd[0][t + s]); sd[1][t] = fmax(sd[1][t], sd[1][t + s]);
+            sd[2][t] = fmin(sd[2][t], sd[2][t + s]); sd[3][t] = fmax(sd[3][t], sd[3][t + s]);
+        }
+        __syncthreads();
+    }
+    mny = sd[0][0]; mxy = sd[1][0]; mnz = sd[2][0]; mxz = sd[3][0];
+    const int none = 0x7fffffff;
+    int fa = none, fb = none, fc = none, fe = none;
+    for (int j = t + 1; j <= ny; j += NT) {
+        if (Y[j] > mny) fa = min(fa, j);
+        if (Y[j] > mxy) fb = min(fb, j);
+    }
+    for (int k = t + 1; k <= nz; k += NT) {
+        if (Z[k] > mnz) fc = min(fc, k);
+        if (Z[k] > mxz) fe = min(fe, k);
+    }
+    si[0][t] = fa; si[1][t] = fb; si[2][t] = fc; si[3][t] = fe;
+    __syncthreads();
+    for (int s = NT / 2; s > 0; s >>= 1) {
+        if (t < s)
+            for (int q = 0; q < 4; ++q) si[q][t] = min(si[q][t], si[q][t + s]);
+        __syncthreads();
+    }
+    if (t == 0) {
+        m.meta[0] = si[0][0] == none ? 0 : si[0][0] - 1;
+        m.meta[1] = si[1][0] == none ? 0 : si[1][0];
+        m.meta[2] = si[2][0] == none ? 0 : si[2][0] - 1;
+        m.meta[3] = si[3][0] == none ? 0 : si[3][0];
+        m.meta[4] = 0;
+        m.meta[5] = 0;
+    }
+}
+
+// Crossing parity of every (k,j) cell; the cut-cell flags cleared.
+__global__ void k_dyn_main(int ny, int nz, const double* Y, const double* Z, DynMask m, const Ctl* ctl) {
+    if (ctl->halt) return;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (k > nz || j > ny) return;
+    const double* az = m.poly;
+    m.flags[(long long)(k - 1) + (long long)nz * (j - 1)] = 0;
+    ray_main_cell(k, j, nz, Y, Z, az, az + m.npts, m.npts, m.eta1, &m.meta[5]);
+}
+
+// Flags of the cells that hold a vertex (within the bounds).
+__global__ void k_dyn_points(int ny, int nz, const double* Y, const double* Z, DynMask m, const Ctl* ctl) {
+    if (ctl->halt) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m.npts) return;
+    const double* az = m.poly;
+    ray_point(q, ny, nz, Y, Z, az, az + m.npts, m.meta[0], m.meta[1], m.meta[2], m.meta[3], m.flags);
+}
+
+// The flagged cells into the list (in any order: each is computed on its own).
+__global__ void k_dyn_compact(int cells, DynMask m, const Ctl* ctl) {
+    if (ctl->halt) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < cells && m.flags[q]) m.list[atomicAdd(&m.meta[4], 1)] = q;
+}
+
+// Sub-cell fractions of the listed cells; blocks stride over the list.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_dyn_sub(int nz, const double* Y, const double* Z, DynMask m,
+                                                const Ctl* ctl) {
+    if (ctl->halt) return;
+    __shared__ int red[NT];
+    const double* az = m.poly;
+    const int count = m.meta[4];
+    for (int q = blockIdx.x; q < count; q += gridDim.x)
+        ray_sub_cell<NT>(m.list[q], nz, Y, Z, az, az + m.npts, m.npts, m.eta1, &m.meta[5], red);
+}
+
+// ETA from ETA_1, as k_extrude.
+__global__ void k_dyn_extrude(Geom g, const double* eta1, double* eta, const Ctl* ctl) {
+    if (ctl->halt) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z - 1;
+    if (i > g.nx + 2 || j > g.ny + 2 || k > g.nz + 2) return;
+    const bool in = i >= 1 && i <= g.nx && j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
+    eta[nat(g, i, j, k)] = in ? eta1[(long long)(k - 1) + (long long)g.nz * (j - 1)] : 0.0;
+}
+
+// The step runs (IF condition 1) unless this or an earlier step of the call met
+// a tie; the first such step's tie count is kept in the control block.
+__global__ void k_dyn_gate(DynMask m, Ctl* ctl, cudaGraphConditionalHandle h) {
+    if (!ctl->halt && m.meta[5] > 0) {
+        ctl->halt = 1;
+        ctl->halt_ties = m.meta[5];
+    }
+    cudaGraphSetConditional(h, ctl->halt ? 0u : 1u);
 }
 
 // DFIB_Cylinder (DFIB.f90:90-131): axis along x, centre (zc, yc), radius r.

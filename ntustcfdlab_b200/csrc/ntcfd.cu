@@ -129,9 +129,19 @@ struct ntcfd_ctx {
     size_t adj_cap = 0;
     long long istep = 0;                    // steps taken by ntcfd_step since ntcfd_create
     // dynamic angle of attack (ntcfd_set_dynamic_aoa); dyn_start = 0: off
-    std::vector<double> dyn_az, dyn_ay;
-    double dyn_aoa1 = 0.0, dyn_rf = 0.0, dyn_zc = 0.0, dyn_yc = 0.0;
+    double dyn_aoa1 = 0.0, dyn_rf = 0.0;
     int dyn_start = 0;
+    // its mask on the device (a second step graph: mask kernels, then the step
+    // under an IF node that a tie switches off)
+    DynMask dyn{};
+    void* dyn_buf = nullptr;                // the DynMask arrays
+    int dyn_cap = 0;                        // polygon points they hold
+    double* dyn_trig = nullptr;             // cos, sin of each step's angle (call-indexed)
+    int dyn_trig_cap = 0;
+    Ctl* ctl_host = nullptr;                // pinned copy of the control block at the end of a call
+    cudaGraph_t graph_dyn = nullptr;
+    cudaGraphExec_t exec_dyn = nullptr;
+    std::string dyn_graph_err;              // why the device path is off (host path used instead)
     // asynchronous output (ntcfd_output_async)
     cudaStream_t out_stream = nullptr;
     cudaEvent_t out_ready = nullptr, out_done = nullptr;
@@ -153,6 +163,19 @@ int fail(ntcfd_ctx* c, int code, const char* fmt, ...) {
     va_end(ap);
     if (c) c->err = buf;
     return code;
+}
+
+// The step graphs hold buffer pointers and the mask flag: any change drops them
+// and the next ntcfd_step rebuilds.
+void drop_dyn_graph(ntcfd_ctx* c) {
+    if (c->exec_dyn) { cudaGraphExecDestroy(c->exec_dyn); c->exec_dyn = nullptr; }
+    if (c->graph_dyn) { cudaGraphDestroy(c->graph_dyn); c->graph_dyn = nullptr; }
+}
+
+void drop_graphs(ntcfd_ctx* c) {
+    if (c->exec) { cudaGraphExecDestroy(c->exec); c->exec = nullptr; }
+    if (c->graph) { cudaGraphDestroy(c->graph); c->graph = nullptr; }
+    drop_dyn_graph(c);
 }
 
 #define CK(call)                                                                          \
@@ -396,13 +419,12 @@ void launch_predictor(ntcfd_ctx* ctx, cudaStream_t st) {
 //   [K1 smag] -> K2 predictor -> K3a rhs -> begin -> WHILE(outer){ defect ->
 //   WHILE(inner){ c x (red, black) -> check } -> correct -> outer_check } ->
 //   K4 project -> K5 columns -> K5 total -> K6 x -> K6 y -> K6 z -> [divmax] -> end
+// The step's nodes added to G (the step graph, or the body of the moving-body
+// graph's IF node); `extra` kernels run before them in the same step.
 template <class Tc>
-int build_graph(ntcfd_ctx* ctx) {
+int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
     const Geom g = ctx->g;
     const ntcfd_params& P = ctx->prm;
-    cudaGraph_t G;
-    GK(cudaGraphCreate(&G, 0));
-    ctx->graph = G;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     std::vector<cudaGraphNode_t> dep;
     cudaGraphNode_t n;
@@ -531,12 +553,70 @@ int build_graph(ntcfd_ctx* ctx) {
     }
     // kernels of a step: predictor, rhs, project, force (2, with a mask), bc (3), step_end, + LES,
     // + diagnostic; + sor_begin and 4 per cycle (streaming) or 2 per solve (resident)
-    const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
+    const int fixed = extra + 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
                       (ctx->resident ? 0 : 1);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
                   P.diag_divergence, fixed, ctx->resident ? 2 : 4, ctx->resident ? 0 : 2 * ctx->csweeps + 1,
                   ctx->mask_nonzero ? 1 : 0, P.lx));
+    return 0;
+}
+
+template <class Tc>
+int build_graph(ntcfd_ctx* ctx) {
+    cudaGraph_t G;
+    GK(cudaGraphCreate(&G, 0));
+    ctx->graph = G;
+    if (int rc = add_step_nodes<Tc>(ctx, G, 0)) return rc;
     GK(cudaGraphInstantiate(&ctx->exec, G, 0));
+    return 0;
+}
+
+// Kernels of the moving body's mask in a step of the moving-body graph.
+constexpr int kDynKernels = 7;
+
+// The moving-body step graph (ntcfd_set_dynamic_aoa): the step's mask
+// (airfoil.f90:311-321, RayCasting at the step's angle) -> gate -> IF(no tie in
+// this call){ the step }.
+template <class Tc>
+int build_dyn_graph(ntcfd_ctx* ctx) {
+    const Geom g = ctx->g;
+    cudaGraph_t G;
+    GK(cudaGraphCreate(&G, 0));
+    ctx->graph_dyn = G;
+    const DynMask m = ctx->dyn;
+    const Ctl* cctl = ctx->ctl;
+    const int cells = g.ny * g.nz;
+    std::vector<cudaGraphNode_t> dep;
+    cudaGraphNode_t n;
+    GK(add_kernel(&n, G, dep, k_dyn_rotate<512>, dim3(1), dim3(512), g.ny, g.nz, (const double*)ctx->coordY,
+                  (const double*)ctx->coordZ, m, cctl));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_dyn_main, dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), g.ny, g.nz,
+                  (const double*)ctx->coordY, (const double*)ctx->coordZ, m, cctl));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_dyn_points, dim3((m.npts + 127) / 128), dim3(128), g.ny, g.nz,
+                  (const double*)ctx->coordY, (const double*)ctx->coordZ, m, cctl));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_dyn_compact, dim3((cells + 255) / 256), dim3(256), cells, m, cctl));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_dyn_sub<256>, dim3(2 * ctx->sm_count), dim3(256), g.nz,
+                  (const double*)ctx->coordY, (const double*)ctx->coordZ, m, cctl));
+    dep = {n};
+    GK(add_kernel(&n, G, dep, k_dyn_extrude, dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2),
+                  dim3(32, 4, 2), g, (const double*)m.eta1, ctx->eta, cctl));
+    dep = {n};
+    cudaGraphConditionalHandle h;
+    GK(cudaGraphConditionalHandleCreate(&h, G, 0, 0));
+    GK(add_kernel(&n, G, dep, k_dyn_gate, dim3(1), dim3(1), m, ctx->ctl, h));
+    dep = {n};
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeIf;
+    np.conditional.size = 1;
+    GK(cudaGraphAddNode(&n, G, dep.data(), dep.size(), &np));
+    if (int rc = add_step_nodes<Tc>(ctx, np.conditional.phGraph_out[0], kDynKernels)) return rc;
+    GK(cudaGraphInstantiate(&ctx->exec_dyn, G, 0));
     return 0;
 }
 
@@ -928,9 +1008,11 @@ void ntcfd_destroy(ntcfd_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-    if (ctx->exec) cudaGraphExecDestroy(ctx->exec);
-    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    drop_graphs(ctx);
     for (void* q : ctx->allocs) cudaFree(q);
+    if (ctx->dyn_trig) cudaFree(ctx->dyn_trig);
+    if (ctx->dyn_buf) cudaFree(ctx->dyn_buf);
+    if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
     if (ctx->rec) cudaFree(ctx->rec);
     if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
     if (ctx->adj_buf) cudaFree(ctx->adj_buf);
@@ -1025,8 +1107,7 @@ int ntcfd_set_metrics(ntcfd_ctx* ctx, const double* iDx, const double* Dxs, cons
     }
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->metrics_set = true;
-    if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
-    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    drop_graphs(ctx);
     return 0;
 }
 
@@ -1049,8 +1130,7 @@ int ntcfd_set_coords(ntcfd_ctx* ctx, const double* X, const double* Y, const dou
 static int set_mask_flag(ntcfd_ctx* ctx, bool nonzero) {
     if (nonzero == ctx->mask_nonzero) return 0;
     CK(cudaStreamSynchronize(ctx->stream));
-    if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
-    if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+    drop_graphs(ctx);
     if (!nonzero) {
         const size_t cols = (size_t)ctx->g.nx * ctx->g.ny;
         CK(cudaMemsetAsync(ctx->FXz, 0, cols * sizeof(double), ctx->stream));
@@ -1157,9 +1237,6 @@ int ntcfd_get_output(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double
 
 }  // extern "C"
 
-extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az_in, const double* ay_in,
-                                                int npts, double aoa, double zc, double yc, int* ties_out);
-
 namespace {
 
 // Limits of the allocation-free mask scratch (defined with the scratch below).
@@ -1172,8 +1249,7 @@ int prepare_steps(ntcfd_ctx* ctx, int nrec) {
     if (nrec > ctx->rec_cap) {
         // the graph holds the record pointer: grow the record buffer, then rebuild
         const int cap = std::max(nrec, 1024);
-        if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
-        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+        drop_graphs(ctx);
         if (ctx->rec) cudaFree(ctx->rec);
         ctx->rec = nullptr;
         ctx->rec_cap = 0;
@@ -1229,8 +1305,11 @@ int records_to_info(ntcfd_ctx* ctx, const StepRec* rec, int nsteps, ntcfd_step_i
 // End of an ntcfd_step call after `ran` steps were launched: the records of
 // those steps come back (into pinned memory: a pageable destination would take
 // the driver's staged, synchronous copy path on every call), the device time
-// of the call, the step count and the simulated time advance by `ran`.
-int finish_steps(ntcfd_ctx* ctx, int ran, ntcfd_step_info* info, const double* aoa) {
+// of the call, the step count and the simulated time advance by `ran`.  With
+// `halted` (moving-body steps on the device), the control block comes back too
+// and the steps that ran are its step count; *halted says whether a tie
+// stopped them.
+int finish_steps(ntcfd_ctx* ctx, int ran, ntcfd_step_info* info, const double* aoa, int* halted = nullptr) {
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     if (ran > ctx->rec_host_cap) {
         if (ctx->rec_host) cudaFreeHost(ctx->rec_host);
@@ -1239,12 +1318,103 @@ int finish_steps(ntcfd_ctx* ctx, int ran, ntcfd_step_info* info, const double* a
         CK(cudaMallocHost(&ctx->rec_host, sizeof(StepRec) * std::max(ran, 1024)));
         ctx->rec_host_cap = std::max(ran, 1024);
     }
+    if (halted) {
+        if (!ctx->ctl_host) CK(cudaMallocHost(&ctx->ctl_host, sizeof(Ctl)));
+        CK(cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, ctx->stream));
+    }
     if (ran > 0)
         CK(cudaMemcpyAsync(ctx->rec_host, ctx->rec, sizeof(StepRec) * ran, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1));
+    if (halted) {
+        *halted = ctx->ctl_host->halt ? ctx->ctl_host->halt_ties : 0;
+        ran = std::min(ran, ctx->ctl_host->step);
+    }
     ctx->istep += ran;
     return records_to_info(ctx, ctx->rec_host, ran, info, aoa);
+}
+
+// The moving body's device arrays for npts polygon points (grown, never
+// shrunk); the polygon goes in as the body's.
+int dyn_alloc(ntcfd_ctx* ctx, const double* az, const double* ay, int npts) {
+    const Geom& g = ctx->g;
+    const size_t cells = (size_t)g.ny * g.nz;
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    if (npts > ctx->dyn_cap) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        drop_dyn_graph(ctx);
+        if (ctx->dyn_buf) cudaFree(ctx->dyn_buf);
+        ctx->dyn_buf = nullptr;
+        ctx->dyn_cap = 0;
+        const size_t bytes = 2 * up(2 * (size_t)npts * sizeof(double)) + up(cells * sizeof(double)) +
+                             2 * up(cells * sizeof(int)) + up(8 * sizeof(int));
+        CK(cudaMalloc(&ctx->dyn_buf, bytes));
+        CK(cudaMemsetAsync(ctx->dyn_buf, 0, bytes, ctx->stream));
+        ctx->dyn_cap = npts;
+    }
+    unsigned char* q = (unsigned char*)ctx->dyn_buf;
+    const size_t pb = up(2 * (size_t)ctx->dyn_cap * sizeof(double));
+    DynMask& m = ctx->dyn;
+    m.base = (const double*)q;
+    m.poly = (double*)(q + pb);
+    m.eta1 = (double*)(q + 2 * pb);
+    m.flags = (int*)(q + 2 * pb + up(cells * sizeof(double)));
+    m.list = (int*)(q + 2 * pb + up(cells * sizeof(double)) + up(cells * sizeof(int)));
+    m.meta = (int*)(q + 2 * pb + up(cells * sizeof(double)) + 2 * up(cells * sizeof(int)));
+    m.trig = ctx->dyn_trig;
+    m.npts = npts;
+    CK(cudaMemcpyAsync((double*)m.base, az, npts * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync((double*)m.base + npts, ay, npts * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// The per-step angle table of a call of nsteps steps and, unless the context
+// is eager or the graph could not be built here, the moving-body step graph.
+int prepare_dyn(ntcfd_ctx* ctx, int nsteps) {
+    if (nsteps > ctx->dyn_trig_cap) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        drop_dyn_graph(ctx);
+        if (ctx->dyn_trig) cudaFree(ctx->dyn_trig);
+        ctx->dyn_trig = nullptr;
+        ctx->dyn_trig_cap = 0;
+        const int cap = std::max(nsteps, 1024);
+        CK(cudaMalloc(&ctx->dyn_trig, 2 * sizeof(double) * cap));
+        ctx->dyn_trig_cap = cap;
+        ctx->dyn.trig = ctx->dyn_trig;
+    }
+    if (ctx->prm.eager || ctx->exec_dyn || !ctx->dyn_graph_err.empty()) return 0;
+    const int rc = ctx->prm.precision == NTCFD_MIXED ? build_dyn_graph<float>(ctx) : build_dyn_graph<double>(ctx);
+    if (rc) {
+        // this device or driver does not take the graph (an IF node around the
+        // step's own loops): the steps launch the mask kernels one by one instead
+        ctx->dyn_graph_err = ctx->err;
+        drop_dyn_graph(ctx);
+        cudaGetLastError();
+    }
+    return 0;
+}
+
+// The mask kernels of a moving-body step launched one by one (eager contexts,
+// or where the moving-body graph could not be built); *ties receives the
+// step's exact vertex/grid ties.
+int dyn_mask_eager(ntcfd_ctx* ctx, int* ties) {
+    const Geom& g = ctx->g;
+    const DynMask m = ctx->dyn;
+    const int cells = g.ny * g.nz;
+    cudaStream_t st = ctx->stream;
+    k_dyn_rotate<512><<<1, 512, 0, st>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, m, ctx->ctl);
+    k_dyn_main<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, st>>>(g.ny, g.nz, ctx->coordY,
+                                                                              ctx->coordZ, m, ctx->ctl);
+    k_dyn_points<<<(m.npts + 127) / 128, 128, 0, st>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, m, ctx->ctl);
+    k_dyn_compact<<<(cells + 255) / 256, 256, 0, st>>>(cells, m, ctx->ctl);
+    k_dyn_sub<256><<<2 * ctx->sm_count, 256, 0, st>>>(g.nz, ctx->coordY, ctx->coordZ, m, ctx->ctl);
+    k_dyn_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), dim3(32, 4, 2), 0, st>>>(
+        g, m.eta1, ctx->eta, ctx->ctl);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(ties, &m.meta[5], sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return 0;
 }
 
 }  // namespace
@@ -1256,35 +1426,65 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     if (nsteps < 0) return fail(ctx, NTCFD_EINVAL, "nsteps < 0");
     if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_step");
     if (nsteps == 0) return 0;
+    // a moving body in this call: its steps rebuild ETA on the device
+    const bool dyn = ctx->dyn_start > 0 && ctx->istep + nsteps >= ctx->dyn_start;
+    if (dyn)
+        if (int rc = set_mask_flag(ctx, true)) return rc;
     if (int rc = prepare_steps(ctx, nsteps)) return rc;
-    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
-    CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    std::vector<double> aoa(nsteps, 0.0);
+    if (dyn)
+        if (int rc = prepare_dyn(ctx, nsteps)) return rc;
+    std::vector<double> aoa(nsteps, 0.0), trig(dyn ? 2 * (size_t)nsteps : 0, 0.0);
     double t = ctx->time;
     for (int s = 0; s < nsteps; ++s) {
         const long long istep = ctx->istep + s + 1;
-        if (ctx->dyn_start > 0 && istep >= ctx->dyn_start) {
+        if (dyn && istep >= ctx->dyn_start) {
             // dynamic_AOA (airfoil.f90:313-317): PI is the default-real literal 3.14159265359
             const double PI = (double)3.14159265359f;
             const double frequency = ctx->dyn_rf / PI;
             aoa[s] = ctx->dyn_aoa1 +
                      10 * std::fabs(std::sin(2 * PI * frequency * (t - ctx->prm.dt * (double)(ctx->dyn_start - 1))));
+            // the rotation of airfoil.f90:597-611 (pi = 4 atan(1) there)
+            const double pr = 4.0 * std::atan(1.0);
+            trig[2 * s] = std::cos((-aoa[s]) * pr / 180);
+            trig[2 * s + 1] = std::sin((-aoa[s]) * pr / 180);
+        }
+        t = t + ctx->prm.dt;
+    }
+    if (dyn) CK(cudaMemcpyAsync(ctx->dyn_trig, trig.data(), trig.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(&ctx->ctl->halt, 0, 2 * sizeof(int), ctx->stream));
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const bool graph_dyn = dyn && ctx->exec_dyn;
+    for (int s = 0; s < nsteps; ++s) {
+        if (dyn && ctx->istep + s + 1 >= ctx->dyn_start) {
+            if (graph_dyn) {
+                CK(cudaGraphLaunch(ctx->exec_dyn, ctx->stream));
+                continue;
+            }
             int ties = 0;
-            const int rc = ntcfd_build_mask_polygon_noalloc(ctx, ctx->dyn_az.data(), ctx->dyn_ay.data(),
-                                                            (int)ctx->dyn_az.size(), aoa[s], ctx->dyn_zc,
-                                                            ctx->dyn_yc, &ties);
-            if (rc) {
+            if (int rc = dyn_mask_eager(ctx, &ties)) return rc;
+            if (ties) {
                 // steps 0..s-1 ran: account for them (time, step count, records) before
                 // returning, so that the host's view matches the device state
-                const std::string why = ctx->err;
                 if (int r2 = finish_steps(ctx, s, info, aoa.data())) return r2;
-                return fail(ctx, rc, "step %lld of this call (%d ran): %s", (long long)s + 1, s, why.c_str());
+                return fail(ctx, NTCFD_EINVAL, "step %d of this call (%d ran): %d exact vertex/grid ties: the "
+                            "reference resolves them by moving the grid", s + 1, s, ties);
             }
         }
         if (int rc = launch_step(ctx)) return rc;
-        t = t + ctx->prm.dt;
     }
-    return finish_steps(ctx, nsteps, info, aoa.data());
+    if (!graph_dyn) return finish_steps(ctx, nsteps, info, aoa.data());
+    int halted = 0;
+    const long long before = ctx->istep;
+    const int rc = finish_steps(ctx, nsteps, info, aoa.data(), &halted);
+    if (halted) {
+        const int ran = (int)(ctx->istep - before);
+        if (rc == 0 || rc == NTCFD_NOT_CONVERGED)
+            return fail(ctx, NTCFD_EINVAL, "step %d of this call (%d ran): %d exact vertex/grid ties: the "
+                        "reference resolves them by moving the grid", ran + 1, ran, halted);
+    }
+    return rc;
 }
 
 int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
@@ -1347,8 +1547,8 @@ int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, in
     DEV();
     if (npts == 0) {
         ctx->dyn_start = 0;
-        ctx->dyn_az.clear();
-        ctx->dyn_ay.clear();
+        CK(cudaStreamSynchronize(ctx->stream));
+        drop_dyn_graph(ctx);
         return 0;
     }
     if (!az || !ay || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
@@ -1356,15 +1556,13 @@ int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, in
     if (!std::isfinite(aoa1) || !std::isfinite(reduce_frequency) || !std::isfinite(zc) || !std::isfinite(yc))
         return fail(ctx, NTCFD_EINVAL, "non-finite dynamic angle parameters");
     if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
-    if (npts > kNaPoly || (size_t)ctx->g.ny * ctx->g.nz > (size_t)kNaCells)
-        return fail(ctx, NTCFD_EINVAL, "the dynamic angle rebuilds the mask without allocating: at most %d "
-                    "polygon points and %d cells in the (k,j) plane", kNaPoly, kNaCells);
-    ctx->dyn_az.assign(az, az + npts);
-    ctx->dyn_ay.assign(ay, ay + npts);
+    CK(cudaStreamSynchronize(ctx->stream));
+    drop_dyn_graph(ctx);     // the graph holds the polygon's size and centre
+    if (int rc = dyn_alloc(ctx, az, ay, npts)) return rc;
+    ctx->dyn.zc = zc;
+    ctx->dyn.yc = yc;
     ctx->dyn_aoa1 = aoa1;
     ctx->dyn_rf = reduce_frequency;
-    ctx->dyn_zc = zc;
-    ctx->dyn_yc = yc;
     ctx->dyn_start = start_step;
     return 0;
 }
@@ -1612,8 +1810,7 @@ extern "C" int ntcfd_set_body_force(ntcfd_ctx* ctx, const double* fu, const doub
         if (ctx->fb) {
             // the graph holds the pointer: drop it so that the next step rebuilds without the force
             CK(cudaStreamSynchronize(ctx->stream));
-            if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
-            if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+            drop_graphs(ctx);
             ctx->fb = nullptr;   // the storage stays in ctx->allocs
         }
         return 0;
@@ -1622,8 +1819,7 @@ extern "C" int ntcfd_set_body_force(ntcfd_ctx* ctx, const double* fu, const doub
         double* q = nullptr;
         if (int rc = dalloc(ctx, &q, 3 * N)) return rc;
         ctx->fb = q;
-        if (ctx->exec) { cudaGraphExecDestroy(ctx->exec); ctx->exec = nullptr; }
-        if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+        drop_graphs(ctx);
     }
     const size_t n = (size_t)g.nx * g.ny * g.nz;
     const double* src[3] = {fu, fv, fw};

@@ -62,6 +62,8 @@ struct Ctl {
     int timeout;                  // a bounded device wait gave up
     int pad_stop, pad_more;       // the last loop decisions (read by the host in eager mode)
     int restarts;                 // correction cycles restarted inside the resident SOR kernel
+    int halt;                     // a moving body's mask met a tie: the call's remaining steps do nothing
+    int halt_ties;                // the ties of that mask
     int pad2;
     double last_change;           // value of the last tested sweep
     double cdrag, clift, divmax;

@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 
 from conftest import interior, rel_l2
-from ntustcfdlab_b200.abi import dptr, f4, make_params, params_copy
+from ntustcfdlab_b200 import abi
+from ntustcfdlab_b200.abi import NtcfdStepInfo, dptr, f4, make_params, params_copy
 
 pytestmark = pytest.mark.gpu
 
@@ -24,18 +25,26 @@ def params():
     return make_params(*N, Re=1000.0, dt=f4(1e-3), bc=bc, bc_value={"Back": (0.0, 0.0, 1.0)}, lx=L[0])
 
 
-def dynamic_aoa(t, dt):
+def dynamic_aoa(t, dt, start=START):
     # airfoil.f90:313-317 with the default-real PI literal
     pi = float(np.float32(3.14159265359))
     frequency = RF / pi
-    return AOA1 + 10 * abs(math.sin(2 * pi * frequency * (t - dt * (START - 1))))
+    return AOA1 + 10 * abs(math.sin(2 * pi * frequency * (t - dt * (start - 1))))
 
 
-def test_dynamic_angle_matches_oracle(orc):
+# the moving-body graph (mask kernels, then the step under an IF node) around
+# the resident and the streaming solve, and the eager launches
+PATHS = [dict(), dict(sor_path=abi.SOR_STREAMING), dict(eager=1)]
+
+
+@pytest.mark.parametrize("path", PATHS, ids=["graph-resident", "graph-streaming", "eager"])
+def test_dynamic_angle_matches_oracle(orc, path):
     from ntustcfdlab_b200.solver import Solver, gridder_unequal, naca4_polygon
     z, y = naca4_polygon(0.12, 64)
     grid = gridder_unequal(*N, *L, BAND)
     p = params()
+    for k, v in path.items():
+        setattr(p, k, v)
     # device
     s = Solver(p, grid)
     try:
@@ -66,6 +75,48 @@ def test_dynamic_angle_matches_oracle(orc):
     assert [i.sor_iters for i in info] == [i.sor_iters for i in oi]
     for k, a in zip("uvwp", state):
         assert rel_l2(interior(a), interior(o.get(k))) <= 1e-12, k
+
+
+@pytest.mark.parametrize("eager", [0, 1])
+def test_a_tie_stops_the_call_after_the_steps_before_it(eager):
+    """A body whose pivot vertex (0.25, 0) sits on a grid node ties at every
+    angle: the call runs the steps before start_step, then stops with
+    NTCFD_EINVAL.  The time, the step count and the records count exactly
+    those steps, ETA holds the tied step's mask (as the allocation-free
+    builder makes it at that angle), and the next call stops at once."""
+    import ctypes
+    from ntustcfdlab_b200.solver import Solver, gridder_equal
+    n, zc, yc, start = (3, 32, 32), 1.0, 2.0, 3
+    p = make_params(*n, Re=100.0, dt=f4(1e-3), eager=eager)
+    s = Solver(p, gridder_equal(*n, 1.0, 4.0, 4.0))
+    z = np.ascontiguousarray([0.25, 0.61, 1.03, 0.58, 0.25])
+    y = np.ascontiguousarray([0.0, 0.37, 0.013, -0.33, 0.0])
+    try:
+        s.set_dynamic_aoa(z, y, AOA1, RF, zc, yc, start)
+        s.boundary_conditions()
+        info = (NtcfdStepInfo * 5)()
+        assert s.lib.ntcfd_step(s.h, 5, info) == abi.NTCFD_EINVAL
+        assert "(2 ran)" in s._err() and "ties" in s._err(), s._err()
+        t = 0.0
+        for _ in range(2):
+            t = t + p.dt
+        assert s.time == t
+        assert info[0].sor_iters > 0 and info[1].sor_iters > 0 and info[2].sor_iters == 0
+        eta = s.get_mask()
+        assert eta.any()
+        ties = ctypes.c_int(-1)
+        assert s.lib.ntcfd_build_mask_polygon_noalloc(s.h, dptr(z), dptr(y), len(z), dynamic_aoa(t, p.dt, start),
+                                                      zc, yc, ctypes.byref(ties)) == abi.NTCFD_EINVAL
+        assert ties.value > 0
+        np.testing.assert_array_equal(s.get_mask(), eta)
+        assert s.lib.ntcfd_step(s.h, 1, info) == abi.NTCFD_EINVAL
+        assert "(0 ran)" in s._err()
+        assert s.time == t
+        s.set_dynamic_aoa(None, None, 0, 0, 0, 0, 0)
+        info2, rc = s.step(1)
+        assert rc == 0 and info2[0].converged and s.time == t + p.dt
+    finally:
+        s.close()
 
 
 def test_adjoint_refuses_a_moving_mask():
