@@ -137,6 +137,49 @@ def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int
     return out
 
 
+def moving_body_cost(name: str = "c3", steps: int = 200, rf: float = 2.0, log=print) -> dict:
+    """Per-step cost of a moving body (ntcfd_set_dynamic_aoa) on an airfoil
+    case, mixed precision, from the case's initial state.  Three runs of the
+    same steps: the static mask; the mask rebuilt every step at the same angle
+    (reduced frequency 0: identical flow and sweeps, so the difference is the
+    mask kernels alone); and a pitching body (reduced frequency rf).  Two
+    untimed steps come first in each (the pitching angles start two steps in)."""
+    fn, _ = WINDOWS[name]
+    out = {"case": name, "steps": steps, "reduce_frequency": rf}
+    for tag, f in (("static", None), ("rebuilt_same_angle", 0.0), ("pitching", rf)):
+        c = fn(precision=MIXED)
+        m = c.mask
+        s = _solver(c)
+        try:
+            st0 = _initial_state(c)
+            if f is not None:
+                s.set_dynamic_aoa(m["az"], m["ay"], m["aoa"], f, m["zc"], m["yc"], 1)
+            s.set_state(*st0)
+            s.boundary_conditions()
+            s.step(2)                       # graph instantiation, outside the timed steps
+            s.set_state(*st0)
+            s.boundary_conditions()
+            info, ms, done = [], 0.0, 0
+            while done < steps:
+                n = min(CHUNK, steps - done)
+                inf, rc = s.step(n)
+                info += inf
+                ms += s.last_step_ms()
+                done += n
+            sw = np.array([i.sor_iters for i in info])
+            out[tag] = {"ms_per_step": ms / steps, "sweeps_per_step": float(sw.mean()),
+                        "launches_per_step": float(np.mean([i.launches for i in info])),
+                        "aoa_min": float(min(i.aoa for i in info)), "aoa_max": float(max(i.aoa for i in info)),
+                        "cLift_last": info[-1].cLift}
+            log(f"  {name} {tag}: {out[tag]}")
+        finally:
+            s.close()
+    st, same = out["static"], out["rebuilt_same_angle"]
+    out["mask_ms_per_step"] = same["ms_per_step"] - st["ms_per_step"]
+    out["same_sweeps"] = st["sweeps_per_step"] == same["sweeps_per_step"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--cases", default="c1,c2,c3,c4,c5")
@@ -144,7 +187,16 @@ def main():
     ap.add_argument("--steps", type=int, default=None, help="override the configured step count")
     ap.add_argument("--adjoint", type=int, default=0, help="C5: adjoint of mean cLift over the last K steps")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--moving", type=int, default=0,
+                    help="instead: per-step cost of a moving body on c3 over this many steps")
     args = ap.parse_args()
+    if args.moving:
+        r = moving_body_cost("c3", args.moving, log=lambda m: print(m, flush=True))
+        print(json.dumps(r), flush=True)
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(r, f, indent=1)
+        return
     res = []
     for name in args.cases.split(","):
         name = name.strip()
