@@ -15,7 +15,14 @@ module ntcfd_iface
    integer(c_int), parameter :: NTCFD_EINVAL = -1, NTCFD_ECUDA = -2, NTCFD_ENOMEM = -3, &
                                 NTCFD_ENONFINITE = -4, NTCFD_ESTATE = -5, NTCFD_ETIMEOUT = -6
    integer(c_int), parameter :: NTCFD_BC_NOSLIP = 0, NTCFD_BC_NEUMANN = 1, &
-                                NTCFD_BC_DIRICHLET = 2, NTCFD_BC_PERIODIC = 3
+                                NTCFD_BC_DIRICHLET = 2, NTCFD_BC_PERIODIC = 3, &
+                                NTCFD_BC_INTERFACE = 4
+   integer(c_int), parameter :: NTCFD_FIELD_U = 0, NTCFD_FIELD_V = 1, NTCFD_FIELD_W = 2, &
+                                NTCFD_FIELD_P = 3, NTCFD_FIELD_WSTAR = 4, NTCFD_FIELD_E_RED = 5, &
+                                NTCFD_FIELD_E_BLACK = 6
+   integer(c_int), parameter :: NTCFD_STAGE_PREDICT = 0, NTCFD_STAGE_RHS = 1, &
+                                NTCFD_STAGE_HALFSWEEP = 2, NTCFD_STAGE_CORRECT = 3, &
+                                NTCFD_STAGE_PROJECT = 4
    integer(c_int), parameter :: NTCFD_WEST = 0, NTCFD_EAST = 1, NTCFD_SOUTH = 2, &
                                 NTCFD_NORTH = 3, NTCFD_BACK = 4, NTCFD_FRONT = 5
    integer(c_int), parameter :: NTCFD_FP64 = 0, NTCFD_MIXED = 1
@@ -209,6 +216,32 @@ module ntcfd_iface
       integer(c_int) function ntcfd_output_wait(ctx) bind(C, name="ntcfd_output_wait")
          import :: c_int, c_ptr
          type(c_ptr), value :: ctx
+      end function
+
+      ! z-slab stages (one context per slab; the caller exchanges the planes)
+      integer(c_int) function ntcfd_slab_stage(ctx, stage, colour) bind(C, name="ntcfd_slab_stage")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: stage, colour
+      end function
+
+      integer(c_int) function ntcfd_slab_change(ctx, max_change) bind(C, name="ntcfd_slab_change")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(out) :: max_change
+      end function
+
+      integer(c_long_long) function ntcfd_slab_plane_elems(ctx, field) bind(C, name="ntcfd_slab_plane_elems")
+         import :: c_int, c_ptr, c_long_long
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: field
+      end function
+
+      ! buf: count * ntcfd_slab_plane_elems doubles (host, or c_loc of device memory)
+      integer(c_int) function ntcfd_slab_planes(ctx, field, k0, count, buf, put) bind(C, name="ntcfd_slab_planes")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx, buf
+         integer(c_int), value :: field, k0, count, put
       end function
 
       ! fu, fv, fw: c_loc of an (nx,ny,nz) array, or c_null_ptr for a zero component

@@ -45,7 +45,9 @@ extern "C" {
 /* Boundary-condition kinds: the strings 'no-slip', 'Neumann', 'Dirichlet'
  * of variables_module.f90:110-132, plus PERIODIC (no reference counterpart). */
 enum { NTCFD_BC_NOSLIP = 0, NTCFD_BC_NEUMANN = 1, NTCFD_BC_DIRICHLET = 2,
-       NTCFD_BC_PERIODIC = 3 };
+       NTCFD_BC_PERIODIC = 3,
+       NTCFD_BC_INTERFACE = 4 /* Back/Front only, all three components: the face is
+                                 shared with the neighbouring z-slab (ntcfd_slab_stage) */ };
 /* Walls, in the order boundary_conditions.f90 applies them (13-301). */
 enum { NTCFD_WEST = 0, NTCFD_EAST = 1, NTCFD_SOUTH = 2, NTCFD_NORTH = 3,
        NTCFD_BACK = 4, NTCFD_FRONT = 5 };
@@ -235,6 +237,44 @@ int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out);
 int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
                           double aoa1, double reduce_frequency, double zc, double yc,
                           int start_step);
+
+/* z-slab decomposition (Mpi_division.f90:6-24): one context (one GPU, one
+ * process) per slab of z planes, created with the slab's nz, the slab's
+ * slice of the z metrics (ghost entries from the neighbours' cells) and
+ * NTCFD_BC_INTERFACE on each face shared with a neighbour.  Such a context
+ * does not take ntcfd_step; the caller runs each step as
+ *     exchange u, v, w (2 planes)                  main.f90:163-183
+ *     NTCFD_STAGE_PREDICT
+ *     exchange w* (1 plane)                        main.f90:220-226
+ *     exchange p (1 plane); NTCFD_STAGE_RHS
+ *     repeat: for the global red then black colour: NTCFD_STAGE_HALFSWEEP
+ *             with the slab's own colour (the global one flipped when the
+ *             slab's first plane has an even global index), then exchange
+ *             that colour's e (1 plane);              GS.f90:20-28
+ *             max over the slabs of ntcfd_slab_change; stop as GS.f90:11
+ *     NTCFD_STAGE_CORRECT; exchange p (1 plane)     main.f90:236-242
+ *     NTCFD_STAGE_PROJECT
+ * where "exchange f (n planes)" moves a slab's first n interior planes of f
+ * into the lower neighbour's top n ghost planes and its last n interior
+ * planes into the upper neighbour's bottom n ghost planes.  The stages run
+ * the FP64 streaming kernels of ntcfd_step, so the decomposed step repeats
+ * the single-domain FP64 streaming step bit for bit.  The force integral is
+ * not formed on slabs.  FP64 contexts only. */
+enum { NTCFD_FIELD_U = 0, NTCFD_FIELD_V = 1, NTCFD_FIELD_W = 2, NTCFD_FIELD_P = 3,
+       NTCFD_FIELD_WSTAR = 4, NTCFD_FIELD_E_RED = 5, NTCFD_FIELD_E_BLACK = 6 };
+enum { NTCFD_STAGE_PREDICT = 0, NTCFD_STAGE_RHS = 1, NTCFD_STAGE_HALFSWEEP = 2,
+       NTCFD_STAGE_CORRECT = 3, NTCFD_STAGE_PROJECT = 4 };
+/* Launches one stage on the context's stream (colour: the half-sweep's
+ * colour in the slab's own indexing, 0 = (i+j+k) even). */
+int ntcfd_slab_stage(ntcfd_ctx* ctx, int stage, int colour);
+/* max |change| of the half-sweeps since the last call (then cleared). */
+int ntcfd_slab_change(ntcfd_ctx* ctx, double* max_change);
+/* Elements of one z plane of a field (natural or colour-split layout). */
+long long ntcfd_slab_plane_elems(const ntcfd_ctx* ctx, int field);
+/* Copies planes k0..k0+count-1 (k in -1..nz+2) of a field out of the
+ * context (put = 0) or into it (put = 1); buf holds count * plane_elems
+ * doubles in host or device memory.  Waits for the copy. */
+int ntcfd_slab_planes(ntcfd_ctx* ctx, int field, int k0, int count, double* buf, int put);
 
 /* The centred output of ntcfd_get_output without waiting for it
  * (filereachtime every isto steps, main.f90:318-324): the fields of the last

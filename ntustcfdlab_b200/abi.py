@@ -23,7 +23,9 @@ NTCFD_ENONFINITE = -4
 NTCFD_ESTATE = -5
 NTCFD_ETIMEOUT = -6
 
-BC_NOSLIP, BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC = 0, 1, 2, 3
+BC_NOSLIP, BC_NEUMANN, BC_DIRICHLET, BC_PERIODIC, BC_INTERFACE = 0, 1, 2, 3, 4
+FIELD_U, FIELD_V, FIELD_W, FIELD_P, FIELD_WSTAR, FIELD_E_RED, FIELD_E_BLACK = range(7)
+STAGE_PREDICT, STAGE_RHS, STAGE_HALFSWEEP, STAGE_CORRECT, STAGE_PROJECT = range(5)
 WEST, EAST, SOUTH, NORTH, BACK, FRONT = 0, 1, 2, 3, 4, 5
 FP64, MIXED = 0, 1
 QUICK_CENTRE, QUICK, UPWIND, CENTRE = 0, 1, 2, 3   # K2 schemes (discretisation_*.f90)
@@ -33,7 +35,7 @@ SOR_AUTO, SOR_STREAMING, SOR_RESIDENT = 0, 1, 2
 
 # boundary-condition strings of variables_module.f90:110-132
 BC_NAMES = {"no-slip": BC_NOSLIP, "Neumann": BC_NEUMANN, "Dirichlet": BC_DIRICHLET,
-            "periodic": BC_PERIODIC}
+            "periodic": BC_PERIODIC, "interface": BC_INTERFACE}
 WALL_NAMES = ("West", "East", "South", "North", "Back", "Front")
 
 
@@ -182,6 +184,11 @@ SIGNATURES = {
     "ntcfd_set_body_force": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 3),
     "ntcfd_set_dynamic_aoa": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int] + [ctypes.c_double] * 4
                               + [ctypes.c_int]),
+    "ntcfd_slab_stage": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    "ntcfd_slab_change": (ctypes.c_int, [ctypes.c_void_p, _DP]),
+    "ntcfd_slab_plane_elems": (ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int]),
+    "ntcfd_slab_planes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_int]),
     "ntcfd_output_async": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),
     "ntcfd_output_wait": (ctypes.c_int, [ctypes.c_void_p]),
     "ntcfd_adjoint": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NtcfdAdjSpec),

@@ -161,7 +161,7 @@ struct BcArgs {
     double *faceB, *faceF;   // w(i,j,0), w(i,j,nz), [(j-1)*nx + i-1]
 };
 
-enum { BC_NOSLIP = 0, BC_NEUMANN = 1, BC_DIRICHLET = 2, BC_PERIODIC = 3 };
+enum { BC_NOSLIP = 0, BC_NEUMANN = 1, BC_DIRICHLET = 2, BC_PERIODIC = 3, BC_INTERFACE = 4 };
 
 // ghost of a tangential component on a wall: 2*val - interior, interior, value, periodic copy
 __device__ __forceinline__ double tangential(int kind, double val, double inner, double periodic_src) {
@@ -328,8 +328,9 @@ __global__ void k_bc_z(Geom g, BcArgs a) {
         a.faceB[f] = a.w[K(0)];
         a.faceF[f] = a.w[K(nz)];
     }
-    // Back (boundary_conditions.f90:205-252): u, v tangential, w normal
-    {
+    // Back (boundary_conditions.f90:205-252): u, v tangential, w normal.  A face
+    // shared with the neighbouring z-slab keeps the planes the exchange wrote.
+    if (a.bc[4][0] != BC_INTERFACE) {
         double* f2[2] = {a.u, a.v};
         for (int c = 0; c < 2; ++c) {
             double* f = f2[c];
@@ -353,7 +354,7 @@ __global__ void k_bc_z(Geom g, BcArgs a) {
         a.w[K(-1)] = (kw == BC_PERIODIC) ? a.w[K(nz - 1)] : w0;
     }
     // Front (boundary_conditions.f90:255-301)
-    {
+    if (a.bc[5][0] != BC_INTERFACE) {
         double* f2[2] = {a.u, a.v};
         for (int c = 0; c < 2; ++c) {
             double* f = f2[c];
@@ -380,8 +381,8 @@ __global__ void k_bc_z(Geom g, BcArgs a) {
         a.p[K(nz + 1)] = a.p[K(1)]; a.p[K(nz + 2)] = a.p[K(2)];
     } else {
         const double p1 = a.p[K(1)], pn = a.p[K(nz)];
-        a.p[K(0)] = p1; a.p[K(-1)] = p1;
-        a.p[K(nz + 1)] = pn; a.p[K(nz + 2)] = pn;
+        if (a.bc[4][2] != BC_INTERFACE) { a.p[K(0)] = p1; a.p[K(-1)] = p1; }
+        if (a.bc[5][2] != BC_INTERFACE) { a.p[K(nz + 1)] = pn; a.p[K(nz + 2)] = pn; }
     }
 }
 

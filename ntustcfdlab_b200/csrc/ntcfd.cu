@@ -167,6 +167,11 @@ int fail(ntcfd_ctx* c, int code, const char* fmt, ...) {
 
 // The step graphs hold buffer pointers and the mask flag: any change drops them
 // and the next ntcfd_step rebuilds.
+// A z-slab context: a Back or Front face is shared with a neighbouring slab.
+bool is_slab(const ntcfd_ctx* c) {
+    return c->prm.bc[NTCFD_BACK][0] == NTCFD_BC_INTERFACE || c->prm.bc[NTCFD_FRONT][0] == NTCFD_BC_INTERFACE;
+}
+
 void drop_dyn_graph(ntcfd_ctx* c) {
     if (c->exec_dyn) { cudaGraphExecDestroy(c->exec_dyn); c->exec_dyn = nullptr; }
     if (c->graph_dyn) { cudaGraphDestroy(c->graph_dyn); c->graph_dyn = nullptr; }
@@ -745,8 +750,12 @@ int validate(const ntcfd_params* p, std::string* why) {
     if (p->LES != 0 && p->LES != 1) return bad("LES must be 0 or 1");
     if (p->check_every < 0 || p->mixed_cycle < 0) return bad("check_every and mixed_cycle must be >= 0");
     for (int wl = 0; wl < 6; ++wl)
-        for (int c = 0; c < 3; ++c)
-            if (p->bc[wl][c] < 0 || p->bc[wl][c] > 3) return bad("bad boundary-condition kind");
+        for (int c = 0; c < 3; ++c) {
+            if (p->bc[wl][c] < 0 || p->bc[wl][c] > NTCFD_BC_INTERFACE) return bad("bad boundary-condition kind");
+            if (p->bc[wl][c] == NTCFD_BC_INTERFACE && (wl < NTCFD_BACK || p->bc[wl][0] != p->bc[wl][1] ||
+                                                       p->bc[wl][0] != p->bc[wl][2]))
+                return bad("NTCFD_BC_INTERFACE: Back or Front walls only, all three components");
+        }
     for (int ax = 0; ax < 3; ++ax) {
         const int lo = 2 * ax, hi = 2 * ax + 1;
         bool any = false, all = true;
@@ -1425,6 +1434,9 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
     DEV();
     if (nsteps < 0) return fail(ctx, NTCFD_EINVAL, "nsteps < 0");
     if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come before ntcfd_step");
+    if (is_slab(ctx))
+        return fail(ctx, NTCFD_EINVAL, "a z-slab context (a Back or Front wall of kind NTCFD_BC_INTERFACE) "
+                    "advances through ntcfd_slab_stage");
     if (nsteps == 0) return 0;
     // a moving body in this call: its steps rebuild ETA on the device
     const bool dyn = ctx->dyn_start > 0 && ctx->istep + nsteps >= ctx->dyn_start;
@@ -1485,6 +1497,127 @@ int ntcfd_step(ntcfd_ctx* ctx, int nsteps, ntcfd_step_info* info) {
                         "reference resolves them by moving the grid", ran + 1, ran, halted);
     }
     return rc;
+}
+
+// ------------------------------------------------------------ z-slabs
+// One process (one GPU) per slab of z planes (Mpi_division.f90:6-24); the
+// caller exchanges the planes between stages as main.f90:163-201,220-240 and
+// GS.f90:20-28 do and takes the max of the sweep changes over the slabs
+// (GS.f90:70).  The stages launch the same kernels as a step of the FP64
+// streaming path, so a decomposed solve repeats the single-domain one bit for
+// bit when the exchanges deliver the neighbours' planes.
+
+static double* slab_field(ntcfd_ctx* ctx, int field, long long* plane) {
+    const Geom& g = ctx->g;
+    *plane = g.pz;
+    switch (field) {
+        case NTCFD_FIELD_U: return ctx->u;
+        case NTCFD_FIELD_V: return ctx->v;
+        case NTCFD_FIELD_W: return ctx->w;
+        case NTCFD_FIELD_P: return ctx->p;
+        case NTCFD_FIELD_WSTAR: return ctx->ws;
+        case NTCFD_FIELD_E_RED: *plane = g.mz; return (double*)ctx->eR;
+        case NTCFD_FIELD_E_BLACK: *plane = g.mz; return (double*)ctx->eB;
+        default: return nullptr;
+    }
+}
+
+long long ntcfd_slab_plane_elems(const ntcfd_ctx* ctx, int field) {
+    if (!ctx || field < NTCFD_FIELD_U || field > NTCFD_FIELD_E_BLACK) return -1;
+    return field >= NTCFD_FIELD_E_RED ? ctx->g.mz : ctx->g.pz;
+}
+
+int ntcfd_slab_planes(ntcfd_ctx* ctx, int field, int k0, int count, double* buf, int put) {
+    DEV();
+    long long plane = 0;
+    double* f = slab_field(ctx, field, &plane);
+    if (!f) return fail(ctx, NTCFD_EINVAL, "unknown field %d", field);
+    if (ctx->prm.precision != NTCFD_FP64) return fail(ctx, NTCFD_EINVAL, "the z-slab stages run in FP64");
+    if (!buf || count < 1 || k0 < -1 || k0 + count - 1 > ctx->g.nz + 2)
+        return fail(ctx, NTCFD_EINVAL, "planes %d..%d outside -1..nz+2", k0, k0 + count - 1);
+    double* dev = f + plane * (long long)(k0 + 1);
+    const size_t bytes = sizeof(double) * (size_t)plane * count;
+    if (put) CK(cudaMemcpyAsync(dev, buf, bytes, cudaMemcpyDefault, ctx->stream));
+    else CK(cudaMemcpyAsync(buf, dev, bytes, cudaMemcpyDefault, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+int ntcfd_slab_stage(ntcfd_ctx* ctx, int stage, int colour) {
+    DEV();
+    if (!ctx->metrics_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_metrics must come first");
+    if (ctx->prm.precision != NTCFD_FP64) return fail(ctx, NTCFD_EINVAL, "the z-slab stages run in FP64");
+    const Geom g = ctx->g;
+    const ntcfd_params& P = ctx->prm;
+    cudaStream_t st = ctx->stream;
+    const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
+    double *eR = (double*)ctx->eR, *eB = (double*)ctx->eB, *dR = (double*)ctx->dR, *dB = (double*)ctx->dB;
+    switch (stage) {
+        case NTCFD_STAGE_PREDICT:   // [Smagorinsky] + predictor: u, v, w with two halo planes
+            launch_predictor(ctx, st);
+            break;
+        case NTCFD_STAGE_RHS:       // rhs, the solve's defect and e = 0: w* and p with one halo plane
+            k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w,
+                                                                        ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
+            k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
+            k_defect<double><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
+                                                (const double*)ctx->rdR, (const double*)ctx->rdB, ctx->ctl, 0, 0,
+                                                nullptr, nullptr, 0, 0);
+            k_clear_e<double><<<g3, b3, 0, st>>>(g, eR, eB);
+            // the ghost planes of e hold the neighbours' last planes of the previous
+            // solve: theirs start from zero too
+            for (double* e : {eR, eB}) {
+                CK(cudaMemsetAsync(e, 0, sizeof(double) * g.mz * 2, st));
+                CK(cudaMemsetAsync(e + g.mz * (g.nz + 2), 0, sizeof(double) * g.mz * 2, st));
+            }
+            CK(cudaMemsetAsync(ctx->slots, 0, sizeof(unsigned long long) * kSpread, st));
+            break;
+        case NTCFD_STAGE_HALFSWEEP: {   // colour 0: (i+j+k) even in the slab's own k; e of the other colour
+            if (colour != 0 && colour != 1) return fail(ctx, NTCFD_EINVAL, "colour must be 0 or 1");
+            const dim3 bs = Sweep<double>::block(), gs = Sweep<double>::grid(g, ctx->sm_count);
+            Sweep<double>::fn<<<gs, bs, 0, st>>>(g, ctx->scd, colour ? eB : eR, colour ? eR : eB,
+                                                 colour ? dB : dR, (const double*)(colour ? ctx->rdB : ctx->rdR),
+                                                 colour, P.omega, ctx->ctl, 0, P.itmax, P.itmax, 0, ctx->slots);
+            break;
+        }
+        case NTCFD_STAGE_CORRECT:   // p += e
+            k_correct<double><<<g3, b3, 0, st>>>(g, ctx->p, eR, eB);
+            break;
+        case NTCFD_STAGE_PROJECT: { // projection, forcing, velocity commit, BCs on the physical faces
+            ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
+                        ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
+            k_project<<<dim3((g.nx + 31) / 32, (g.ny + 3) / 4, ctx->nchunk), dim3(32, 4, 1), 0, st>>>(g, pj);
+            BcArgs ba{};
+            ba.u = ctx->u; ba.v = ctx->v; ba.w = ctx->w; ba.p = ctx->p;
+            std::memcpy(ba.bc, P.bc, sizeof ba.bc);
+            std::memcpy(ba.val, P.bc_value, sizeof ba.val);
+            ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
+            ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
+            k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+            k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+            k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+            ctx->time = ctx->time + P.dt;
+            ctx->istep += 1;
+            break;
+        }
+        default:
+            return fail(ctx, NTCFD_EINVAL, "unknown stage %d", stage);
+    }
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int ntcfd_slab_change(ntcfd_ctx* ctx, double* max_change) {
+    DEV();
+    if (!max_change) return fail(ctx, NTCFD_EINVAL, "null max_change");
+    unsigned long long h[kSpread];
+    CK(cudaMemcpyAsync(h, ctx->slots, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemsetAsync(ctx->slots, 0, sizeof h, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long m = 0;
+    for (int q = 0; q < kSpread; ++q) m = h[q] > m ? h[q] : m;
+    std::memcpy(max_change, &m, sizeof m);   // |change| as its bit pattern; NaN stays NaN
+    return 0;
 }
 
 int ntcfd_output_async(ntcfd_ctx* ctx, double* pre, double* uc, double* vc, double* wc) {
@@ -2164,6 +2297,7 @@ extern "C" int ntcfd_adjoint(ntcfd_ctx* ctx, const ntcfd_adj_spec* spec, ntcfd_a
     if (spec->nsteps < 1) return fail(ctx, NTCFD_EINVAL, "nsteps must be >= 1");
     if (ctx->dyn_start > 0)
         return fail(ctx, NTCFD_EINVAL, "the adjoint holds ETA fixed: switch the dynamic angle of attack off");
+    if (is_slab(ctx)) return fail(ctx, NTCFD_EINVAL, "the adjoint runs on a single domain, not on a z-slab");
     if (ctx->prm.scheme != NTCFD_QUICK_CENTRE)
         return fail(ctx, NTCFD_EINVAL, "the adjoint differentiates the NTCFD_QUICK_CENTRE predictor only");
     if (spec->checkpoint_every < 1) return fail(ctx, NTCFD_EINVAL, "checkpoint_every must be >= 1");
