@@ -114,11 +114,13 @@ __device__ __forceinline__ void walk_range(const Geom& g, int& k0, int& k1) {
 
 // K3a -- b' on the interior from the predicted velocity (GS.f90:39-41).
 // u*(0,j,k), v*(i,0,k), w*(i,j,0) equal the state's ghosts (the reference
-// copies u into u_star over the whole halo array in boundary_conditions.f90:317-319).
+// copies u into u_star over the whole halo array in boundary_conditions.f90:317-319),
+// except w*(i,j,0) of a z-slab whose Back face is shared (back_iface): that plane
+// is the lower neighbour's last plane of w* (main.f90:220-226).
 __global__ void __launch_bounds__(kWalkBX * kWalkBY) k_rhs(Geom g, SorCoef<double> sc, const double* u,
                                                           const double* v, const double* w, const double* us,
                                                           const double* vs, const double* ws, double* b,
-                                                          double dt) {
+                                                          double dt, int back_iface) {
     const int i = blockIdx.x * kWalkBX + threadIdx.x + 1;
     const int j = blockIdx.y * kWalkBY + threadIdx.y + 1;
     if (i > g.nx || j > g.ny) return;
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(kWalkBX * kWalkBY) k_rhs(Geom g, SorCoef<doubl
     const double sew = sc.cE[i] + sc.cW[i], sns = sc.cN[j] + sc.cS[j];
     const double rx = g.riDx[i], ry = g.riDy[j];
     const long long cb = nat(g, i, j, k0);
-    double wb = (k0 == 1) ? w[cb - g.pz] : ws[cb - g.pz];
+    double wb = (k0 == 1 && !back_iface) ? w[cb - g.pz] : ws[cb - g.pz];
 #pragma unroll kWalkUnroll
     for (int k = k0; k <= k1; ++k) {
         const long long c = cb + (long long)(k - k0) * g.pz;

@@ -172,6 +172,8 @@ bool is_slab(const ntcfd_ctx* c) {
     return c->prm.bc[NTCFD_BACK][0] == NTCFD_BC_INTERFACE || c->prm.bc[NTCFD_FRONT][0] == NTCFD_BC_INTERFACE;
 }
 
+int back_iface(const ntcfd_ctx* c) { return c->prm.bc[NTCFD_BACK][0] == NTCFD_BC_INTERFACE ? 1 : 0; }
+
 void drop_dyn_graph(ntcfd_ctx* c) {
     if (c->exec_dyn) { cudaGraphExecDestroy(c->exec_dyn); c->exec_dyn = nullptr; }
     if (c->graph_dyn) { cudaGraphDestroy(c->graph_dyn); c->graph_dyn = nullptr; }
@@ -456,7 +458,7 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
     dep = {n};
     GK(add_kernel(&n, G, dep, k_rhs, walk_grid(g, ctx->sm_count), walk_block(), g, ctx->scd, (const double*)ctx->u,
                   (const double*)ctx->v, (const double*)ctx->w, (const double*)ctx->us,
-                  (const double*)ctx->vs, (const double*)ctx->ws, ctx->b, P.dt));
+                  (const double*)ctx->vs, (const double*)ctx->ws, ctx->b, P.dt, back_iface(ctx)));
     dep = {n};
     ctx->resident = false;
     if (P.sor_path != NTCFD_SOR_STREAMING) {
@@ -702,7 +704,7 @@ int run_step_eager(ntcfd_ctx* ctx) {
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
     launch_predictor(ctx, st);
-    k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
+    k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt, back_iface(ctx));
     Ctl h{};
     if (int rc = sor_solve_eager<Tc>(ctx, ctx->p, ctx->b, P.zeta, P.itmax, P.omega, &h)) return rc;
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
@@ -826,7 +828,7 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
         return rc;
     if ((rc = timed([&] {
              k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, ctx->stream>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs,
-                                               ctx->ws, ctx->b, P.dt);
+                                               ctx->ws, ctx->b, P.dt, back_iface(ctx));
          }, &out->rhs_ms, 1)))
         return rc;
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
@@ -1554,11 +1556,16 @@ int ntcfd_slab_stage(ntcfd_ctx* ctx, int stage, int colour) {
     double *eR = (double*)ctx->eR, *eB = (double*)ctx->eB, *dR = (double*)ctx->dR, *dB = (double*)ctx->dB;
     switch (stage) {
         case NTCFD_STAGE_PREDICT:   // [Smagorinsky] + predictor: u, v, w with two halo planes
+            // the reference-aliased Smagorinsky reads storage offsets of the whole
+            // domain's arrays (smagorinsky.f90 with the arrays' declared shape), which a
+            // slab does not hold
+            if (is_slab(ctx) && P.LES && P.smag_mode == NTCFD_SMAG_REF_ALIASED)
+                return fail(ctx, NTCFD_EINVAL, "z-slabs take LES with smag_mode = NTCFD_SMAG_STAGGERED");
             launch_predictor(ctx, st);
             break;
         case NTCFD_STAGE_RHS:       // rhs, the solve's defect and e = 0: w* and p with one halo plane
             k_rhs<<<walk_grid(g, ctx->sm_count), walk_block(), 0, st>>>(g, ctx->scd, ctx->u, ctx->v, ctx->w,
-                                                                        ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt);
+                                                                        ctx->us, ctx->vs, ctx->ws, ctx->b, P.dt, back_iface(ctx));
             k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, P.itmax, 0, 0);
             k_defect<double><<<g3, b3, 0, st>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
                                                 (const double*)ctx->rdR, (const double*)ctx->rdB, ctx->ctl, 0, 0,

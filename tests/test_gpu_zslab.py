@@ -28,8 +28,8 @@ def _params():
     bc = {"West": ("periodic",) * 3, "East": ("periodic",) * 3,
           "South": ("Neumann",) * 3, "North": ("Neumann",) * 3,
           "Back": ("Dirichlet", "Dirichlet", "Dirichlet"), "Front": ("Neumann",) * 3}
-    return abi.make_params(*N, Re=500.0, dt=abi.f4(2e-3), LES=1, bc=bc, bc_value={"Back": (0.0, 0.0, 1.0)},
-                           sor_path=abi.SOR_STREAMING, zeta=1e-8)
+    return abi.make_params(*N, Re=500.0, dt=abi.f4(2e-3), LES=1, smag_mode=abi.SMAG_STAGGERED, bc=bc,
+                           bc_value={"Back": (0.0, 0.0, 1.0)}, sor_path=abi.SOR_STREAMING, zeta=1e-8)
 
 
 def _grid():
@@ -108,7 +108,7 @@ def test_slabs_repeat_the_single_domain_step(tmp_path, world):
         assert np.array_equal(got, a[2:-2, 2:-2, 2:-2]), k
 
 
-def test_slab_contexts_refuse_ntcfd_step_and_mixed_precision():
+def test_slab_contexts_refuse_ntcfd_step_mixed_precision_and_the_aliased_smagorinsky():
     from ntustcfdlab_b200.solver import NtcfdError, Solver
     p = zslab.slab_params(_params(), 1, 3, 3)
     s = Solver(p, zslab.slab_grid(_grid(), 5, 7))
@@ -122,8 +122,9 @@ def test_slab_contexts_refuse_ntcfd_step_and_mixed_precision():
             == abi.NTCFD_EINVAL                      # planes 3..6: past nz + 2 = 5
     finally:
         s.close()
-    m = Solver(abi.params_copy(p, precision=abi.MIXED), zslab.slab_grid(_grid(), 5, 7))
-    try:
-        assert m.lib.ntcfd_slab_stage(m.h, abi.STAGE_PREDICT, 0) == abi.NTCFD_EINVAL
-    finally:
-        m.close()
+    for change in (dict(precision=abi.MIXED), dict(smag_mode=abi.SMAG_REF_ALIASED)):
+        m = Solver(abi.params_copy(p, **change), zslab.slab_grid(_grid(), 5, 7))
+        try:
+            assert m.lib.ntcfd_slab_stage(m.h, abi.STAGE_PREDICT, 0) == abi.NTCFD_EINVAL
+        finally:
+            m.close()
