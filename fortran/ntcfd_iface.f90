@@ -71,6 +71,7 @@ module ntcfd_iface
       real(c_double) :: forward_ms, total_ms, recompute_ms, solve_ms
       integer(c_long_long) :: adj_sweeps
       integer(c_int) :: adj_unconverged, recomputed_steps, fwd_status, pad
+      real(c_double) :: dJ_daoa_body
    end type ntcfd_adj_result
 
    interface
@@ -138,6 +139,15 @@ module ntcfd_iface
          integer(c_int), value :: npts
          real(c_double), value :: aoa, zc, yc
          integer(c_int), intent(out) :: ties
+      end function
+
+      integer(c_int) function ntcfd_build_mask_smooth(ctx, az, ay, npts, aoa_deg, zc, yc, width) &
+            bind(C, name="ntcfd_build_mask_smooth")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: az(*), ay(*)
+         integer(c_int), value :: npts
+         real(c_double), value :: aoa_deg, zc, yc, width
       end function
 
       integer(c_int) function ntcfd_build_mask_cylinder(ctx, zc, yc, r) &

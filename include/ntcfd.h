@@ -153,6 +153,18 @@ int ntcfd_get_mask(ntcfd_ctx* ctx, double* eta);
  * the reference resolves by moving the grid (airfoil.f90:700-702). */
 int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
                              double aoa_deg, double zc, double yc, int* ties_out);
+/* A smoothed, differentiable mask of the same body, for gradients with
+ * respect to its angle of attack (no counterpart in the reference).  The
+ * polygon is moved exactly as ntcfd_build_mask_polygon moves it
+ * (airfoil.f90:597-611); each cell's ETA is a C1 ramp of the signed distance
+ * d (negative inside) from its (y,z) centre to the polygon: with
+ * tau = -d / width, ETA = 1 for tau >= 1, 0 for tau <= -1 and
+ * 0.5 + 0.75 tau - 0.25 tau^3 between (so the mask is the ray-cast body
+ * blurred over +-width).  The context keeps dETA/dAOA, and ntcfd_adjoint then
+ * also reports dJ/dAOA through the rotating body (dJ_daoa_body).  Any other
+ * mask call replaces it. */
+int ntcfd_build_mask_smooth(ntcfd_ctx* ctx, const double* az, const double* ay, int npts,
+                            double aoa_deg, double zc, double yc, double width);
 /* Same result as ntcfd_build_mask_polygon, for callers that must not
  * allocate device memory after set-up.  No counterpart in the reference.
  *
@@ -332,6 +344,8 @@ typedef struct ntcfd_adj_result {
     int recomputed_steps;    /* forward steps re-run from checkpoints */
     int fwd_status;          /* status of the forward pass (0 or NTCFD_NOT_CONVERGED) */
     int pad;
+    double dJ_daoa_body;     /* dJ / d(the body's angle of attack), per radian, through the body's
+                                rotation, when ETA is the mask of ntcfd_build_mask_smooth; else 0 */
 } ntcfd_adj_result;
 
 /* Discrete adjoint of K steps.  Runs the K steps forward from the current

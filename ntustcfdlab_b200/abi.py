@@ -99,6 +99,7 @@ class NtcfdAdjResult(ctypes.Structure):
         ("recompute_ms", ctypes.c_double), ("solve_ms", ctypes.c_double),
         ("adj_sweeps", ctypes.c_longlong), ("adj_unconverged", ctypes.c_int),
         ("recomputed_steps", ctypes.c_int), ("fwd_status", ctypes.c_int), ("pad", ctypes.c_int),
+        ("dJ_daoa_body", ctypes.c_double),
     ]
 
 
@@ -169,6 +170,7 @@ SIGNATURES = {
     "ntcfd_build_mask_polygon_noalloc": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int,
                                                         ctypes.c_double, ctypes.c_double,
                                                         ctypes.c_double, _IP]),
+    "ntcfd_build_mask_smooth": (ctypes.c_int, [ctypes.c_void_p, _DP, _DP, ctypes.c_int] + [ctypes.c_double] * 4),
     "ntcfd_build_mask_cylinder": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double,
                                                  ctypes.c_double, ctypes.c_double]),
     "ntcfd_set_state": (ctypes.c_int, [ctypes.c_void_p] + [_DP] * 4),

@@ -554,6 +554,41 @@ __global__ void k_adj_project1(Geom g, double* lu, double* lv, double* lw, const
     lw[c] = 0.0;
 }
 
+// dJ/dETA of one step, accumulated into geta: ETA enters u2 = (1 - eta) u1 + eta us
+// (likewise v, w) and the force integrands FY = eta (vs - v1)/dt, FZ = eta (ws - w1)/dt,
+// with u1 = u* - dt (p(i+1) - p(i))/Dxs(i): p^{n+1} inside (pn), the frozen ghosts of
+// p^n at i = nx+1, j = ny+1, k = nz+1 (po), as k_project reads them.  lu, lv, lw hold
+// lam of u2 after the boundary-condition transpose, wD and wL dJ/dFZ and dJ/dFY.
+__global__ void k_adj_eta(Geom g, const double* lu, const double* lv, const double* lw, const double* wD,
+                          const double* wL, const double* us, const double* vs, const double* ws,
+                          const double* pn, const double* po, double usol, double vsol, double wsol, double dt,
+                          double* geta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long c = nat(g, i, j, k);
+    const double pc = pn[c];
+    const double pe = (i == g.nx ? po : pn)[c + 1];
+    const double pnn = (j == g.ny ? po : pn)[c + g.px];
+    const double pf = (k == g.nz ? po : pn)[c + g.pz];
+    const double u1 = us[c] - dt * (pe - pc) * g.rDxs[i];
+    const double v1 = vs[c] - dt * (pnn - pc) * g.rDys[j];
+    const double w1 = ws[c] - dt * (pf - pc) * g.rDzs[k];
+    geta[c] += lu[c] * (usol - u1) + lv[c] * (vsol - v1) + lw[c] * (wsol - w1) +
+               (wL[c] * (vsol - v1) + wD[c] * (wsol - w1)) / dt;
+}
+
+// Column sums over i of a natural-layout field into a (k,j) plane (k fastest).
+__global__ void k_colsum_i(Geom g, const double* f, double* plane) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (k > g.nz || j > g.ny) return;
+    double s = 0.0;
+    for (int i = 1; i <= g.nx; ++i) s += f[nat(g, i, j, k)];
+    plane[(long long)(k - 1) + (long long)g.nz * (j - 1)] = s;
+}
+
 // lam_p of p^{n+1} (interior, gathered) and of the frozen ghosts of p^n
 // (i = nx+1, j = ny+1, k = nz+1) from lam_u1 = lus etc.
 __global__ void k_adj_project2(Geom g, const double* lus, const double* lvs, const double* lws, double dt,

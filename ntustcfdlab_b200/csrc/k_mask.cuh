@@ -157,6 +157,60 @@ __global__ void k_extrude(Geom g, const double* eta1, double* eta) {
     eta[nat(g, i, j, k)] = in ? eta1[(long long)(k - 1) + (long long)g.nz * (j - 1)] : 0.0;
 }
 
+// ---- A smoothed, differentiable mask (no counterpart in the reference): the
+// polygon moved as the ray cast moves it, ETA_1 a C1 ramp of the signed
+// distance d from the (y,z) cell centre to the polygon (negative inside):
+//     tau = -d / width,  ETA_1 = 1 (tau >= 1), 0 (tau <= -1),
+//     0.5 + 0.75 tau - 0.25 tau^3 between,
+// and dETA_1/dalpha from the vertices' derivatives (dpz, dpy) with respect to
+// the angle: d is the distance to the nearest point Q = A + t (B - A) of the
+// nearest edge, so dd/dalpha = -s n.((1 - t) dA + t dB), n the unit vector
+// from Q to the centre, s = -1 inside.  Inside/outside by crossing parity.
+__global__ void k_smooth_mask(int ny, int nz, const double* Y, const double* Z, const double* pz,
+                              const double* py, const double* dpz, const double* dpy, int npts, double width,
+                              double* eta1, double* deta1) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (k > nz || j > ny) return;
+    const double yc = (Y[j] + Y[j + 1]) / 2.0, zc = (Z[k] + Z[k + 1]) / 2.0;
+    double best = INFINITY, bt = 0.0;
+    int bm = 0;
+    bool inside = false;
+    for (int m = 0; m < npts - 1; ++m) {
+        const double az = pz[m], ay = py[m], bz = pz[m + 1], by = py[m + 1];
+        const double abz = bz - az, aby = by - ay, apz = zc - az, apy = yc - ay;
+        const double l2 = abz * abz + aby * aby;
+        const double t = l2 > 0.0 ? fmin(fmax((apz * abz + apy * aby) / l2, 0.0), 1.0) : 0.0;
+        const double qz = zc - (az + t * abz), qy = yc - (ay + t * aby);
+        const double d2 = qz * qz + qy * qy;
+        if (d2 < best) { best = d2; bt = t; bm = m; }
+        if ((ay > yc) != (by > yc)) {
+            const double zi = az + (yc - ay) * abz / aby;
+            if (zc < zi) inside = !inside;
+        }
+    }
+    const double du = sqrt(best), sgn = inside ? -1.0 : 1.0;
+    const double tau = -sgn * du / width;
+    double e, de = 0.0;
+    if (tau >= 1.0) e = 1.0;
+    else if (tau <= -1.0) e = 0.0;
+    else {
+        e = 0.5 + 0.75 * tau - 0.25 * tau * tau * tau;
+        if (du > 0.0) {
+            const double az = pz[bm], ay = py[bm];
+            const double qz = az + bt * (pz[bm + 1] - az), qy = ay + bt * (py[bm + 1] - ay);
+            const double nz_ = (zc - qz) / du, ny_ = (yc - qy) / du;
+            const double dqz = (1.0 - bt) * dpz[bm] + bt * dpz[bm + 1];
+            const double dqy = (1.0 - bt) * dpy[bm] + bt * dpy[bm + 1];
+            const double ddu = -(nz_ * dqz + ny_ * dqy);
+            de = 0.75 * (1.0 - tau * tau) * (-sgn * ddu / width);
+        }
+    }
+    const long long q = (long long)(k - 1) + (long long)nz * (j - 1);
+    eta1[q] = e;
+    deta1[q] = de;
+}
+
 // ---- The mask of a moving body on the device, one step at a time inside the
 // step graph (ntcfd_set_dynamic_aoa).  The host evaluates each step's angle
 // (airfoil.f90:313-317) and its cosine and sine; k_dyn_rotate turns the body

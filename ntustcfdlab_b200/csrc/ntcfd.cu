@@ -122,6 +122,8 @@ struct ntcfd_ctx {
     float last_ms = 0.0f;
     bool metrics_set = false, coords_set = false;
     bool mask_nonzero = false;              // ETA may be nonzero: the force kernels run
+    double* deta_daoa = nullptr;            // ntcfd_build_mask_smooth: dETA_1/dAOA (ny*nz), per radian
+    bool smooth_active = false;             // ETA is the smoothed mask that deta_daoa belongs to
     double time = 0.0;
     int nchunk = 0, csweeps = 1, cycle_len = 1;
     std::vector<void*> allocs;
@@ -1168,6 +1170,7 @@ static int copy_halo(ntcfd_ctx* ctx, double* dev, const double* host, bool to_de
 
 int ntcfd_set_mask(ntcfd_ctx* ctx, const double* eta) {
     DEV();
+    ctx->smooth_active = false;
     if (!eta) return fail(ctx, NTCFD_EINVAL, "null ETA");
     int rc = copy_halo(ctx, ctx->eta, eta, true);
     if (rc) return rc;
@@ -1696,6 +1699,7 @@ int ntcfd_set_dynamic_aoa(ntcfd_ctx* ctx, const double* az, const double* ay, in
     if (!std::isfinite(aoa1) || !std::isfinite(reduce_frequency) || !std::isfinite(zc) || !std::isfinite(yc))
         return fail(ctx, NTCFD_EINVAL, "non-finite dynamic angle parameters");
     if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    ctx->smooth_active = false;
     CK(cudaStreamSynchronize(ctx->stream));
     drop_dyn_graph(ctx);     // the graph holds the polygon's size and centre
     if (int rc = dyn_alloc(ctx, az, ay, npts)) return rc;
@@ -1725,6 +1729,7 @@ int ntcfd_time_kernels(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
 // ------------------------------------------------------------------ masks
 int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r) {
     DEV();
+    ctx->smooth_active = false;
     if (!ctx->metrics_set || !ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "metrics and coordinates first");
     if (int rc = set_mask_flag(ctx, true)) return rc;
     const Geom& g = ctx->g;
@@ -1739,9 +1744,60 @@ int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r) {
     return 0;
 }
 
+int ntcfd_build_mask_smooth(ntcfd_ctx* ctx, const double* az_in, const double* ay_in, int npts, double aoa,
+                            double zc, double yc, double width) {
+    DEV();
+    ctx->smooth_active = false;
+    if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
+    if (!(width > 0) || !std::isfinite(aoa) || !std::isfinite(zc) || !std::isfinite(yc))
+        return fail(ctx, NTCFD_EINVAL, "width must be positive, the angle and centre finite");
+    if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
+    if (int rc = set_mask_flag(ctx, true)) return rc;
+    const Geom& g = ctx->g;
+    const size_t cells = (size_t)g.ny * g.nz;
+    // the vertices moved as ntcfd_build_mask_polygon moves them (airfoil.f90:597-611), and
+    // their derivatives with respect to the angle in radians (phi = -angle):
+    //   z1 = c z0 - s y0, y1 = s z1 + c y0 (the new z1: the reference's order)
+    std::vector<double> h(4 * (size_t)npts);
+    const double PI = 4.0 * std::atan(1.0);
+    const double c = std::cos((-aoa) * PI / 180), sn = std::sin((-aoa) * PI / 180);
+    for (int i = 0; i < npts; ++i) {
+        const double z0 = az_in[i] - 0.25, y0 = ay_in[i];
+        const double z1 = c * z0 - sn * y0;
+        const double y1 = sn * z1 + c * y0;
+        const double dz1 = -sn * z0 - c * y0;            // d/dphi
+        const double dy1 = c * z1 + sn * dz1 - sn * y0;
+        h[i] = z1 + zc + 0.25;
+        h[npts + i] = y1 + yc;
+        h[2 * npts + i] = -dz1;                          // d/dangle = -d/dphi
+        h[3 * npts + i] = -dy1;
+    }
+    if (!ctx->deta_daoa) {
+        double* q = nullptr;
+        if (int rc = dalloc(ctx, &q, cells)) return rc;
+        ctx->deta_daoa = q;
+    }
+    double* dp = nullptr;
+    CK(cudaMalloc(&dp, sizeof(double) * 4 * npts));
+    CK(cudaMemcpyAsync(dp, h.data(), sizeof(double) * 4 * npts, cudaMemcpyHostToDevice, ctx->stream));
+    double* eta1 = ctx->outbuf;
+    k_smooth_mask<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
+        g.ny, g.nz, ctx->coordY, ctx->coordZ, dp, dp + npts, dp + 2 * npts, dp + 3 * npts, npts, width, eta1,
+        ctx->deta_daoa);
+    const dim3 b3(32, 4, 2);
+    k_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), b3, 0, ctx->stream>>>(
+        g, eta1, ctx->eta);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(dp);
+    ctx->smooth_active = true;
+    return 0;
+}
+
 int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* ay_in, int npts,
                              double aoa, double zc, double yc, int* ties_out) {
     DEV();
+    ctx->smooth_active = false;
     if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
     if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
     if (int rc = set_mask_flag(ctx, true)) return rc;
@@ -1862,6 +1918,7 @@ int noalloc_scratch(ntcfd_ctx* ctx, unsigned char** out) {
 extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az_in, const double* ay_in,
                                                 int npts, double aoa, double zc, double yc, int* ties_out) {
     DEV();
+    ctx->smooth_active = false;
     if (!az_in || !ay_in || npts < 3) return fail(ctx, NTCFD_EINVAL, "polygon needs >= 3 points");
     if (!ctx->coords_set) return fail(ctx, NTCFD_ESTATE, "ntcfd_set_coords must come first");
     const Geom& g = ctx->g;
@@ -1998,6 +2055,7 @@ struct AdjCarve {
 
 struct AdjBufs {
     double *lu, *lv, *lw, *lp, *lpn, *lus, *lvs, *lws, *z, *zprev, *badj, *lb, *wD, *wL, *lnut, *gf, *gval;
+    double *geta, *etacol;       // dJ/dETA summed over the steps, its column sums (smoothed mask only)
     unsigned long long* slot;
     int solves;                  // adjoint solves done (the guess extrapolates after two)
     cudaEvent_t e0, e1;          // around each solve
@@ -2006,11 +2064,12 @@ struct AdjBufs {
 
 // Reverse of one step: on entry lu, lv, lw, lp hold the adjoint of the state
 // after the step; on return the adjoint of the state before it.  (su, sv, sw)
-// is the velocity before the step, `guards` the step's force-integral guards.
+// is the velocity before the step, `guards` the step's force-integral guards;
+// with A.geta, po and pn are the pressure before and after the step.
 template <class Tc>
 int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv, const double* sw,
-                 const unsigned char* guards, double scaleD, double scaleL, double zeta_rel, int itmax,
-                 double omega, long long* sweeps, int* unconverged) {
+                 const double* po, const double* pn, const unsigned char* guards, double scaleD, double scaleL,
+                 double zeta_rel, int itmax, double omega, long long* sweeps, int* unconverged) {
     const Geom g = ctx->g;
     const ntcfd_params& P = ctx->prm;
     cudaStream_t st = ctx->stream;
@@ -2026,6 +2085,15 @@ int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv,
     k_adj_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ab);
     k_adj_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ab);
     k_adj_weights<<<g3, b3, 0, st>>>(g, guards, scaleD, scaleL, A.wD, A.wL);
+    if (A.geta) {
+        // u* of the step again (the forward predictor on the state before it), for u1
+        CK(cudaMemcpyAsync(ctx->u, su, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->v, sv, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemcpyAsync(ctx->w, sw, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        launch_predictor(ctx, st);
+        k_adj_eta<<<g3, b3, 0, st>>>(g, A.lu, A.lv, A.lw, A.wD, A.wL, ctx->us, ctx->vs, ctx->ws, pn, po,
+                                     P.u_solid[0], P.u_solid[1], P.u_solid[2], P.dt, A.geta);
+    }
     k_adj_project1<<<g3, b3, 0, st>>>(g, A.lu, A.lv, A.lw, ctx->eta, A.wD, A.wL, P.dt, A.lus, A.lvs, A.lws);
     k_adj_project2<<<g3, b3, 0, st>>>(g, A.lus, A.lvs, A.lws, P.dt, A.lp, A.lpn);
     k_adj_solve_rhs<<<g3, b3, 0, st>>>(g, ctx->scd, A.lp, A.badj);
@@ -2103,13 +2171,16 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     double *ckpt, *blk, *fin;
     unsigned char* guards;
     AdjBufs A{};
+    // with the smoothed mask the steps' pressures are kept too (dJ/dETA needs u1)
+    const bool body = ctx->smooth_active;
+    const size_t bw = body ? 4 : 3;
     A.e0 = ev.a;
     A.e1 = ev.b;
     double** lam[] = {&A.lu, &A.lv, &A.lw, &A.lp, &A.lpn, &A.lus, &A.lvs, &A.lws, &A.z, &A.zprev, &A.badj,
                       &A.lb, &A.wD, &A.wL};
     auto carve = [&](AdjCarve& cv) {
         cv.take(&ckpt, (size_t)nck * 4 * N);
-        cv.take(&blk, (size_t)M * 3 * N);
+        cv.take(&blk, (size_t)M * bw * N);
         cv.take(&fin, 4 * N + nface);
         cv.take(&guards, (size_t)K * G);
         for (double** q : lam) cv.take(q, N);
@@ -2117,6 +2188,8 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         cv.take(&A.gf, 3 * N);
         cv.take(&A.gval, 18);
         cv.take(&A.slot, 1);
+        cv.take(&A.geta, body ? N : 1);
+        cv.take(&A.etacol, body ? (size_t)g.ny * g.nz : 1);
     };
     {
         AdjCarve sizing;
@@ -2137,6 +2210,8 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     }
     for (double** q : lam) CK(cudaMemsetAsync(*q, 0, N * sizeof(double), st));
     CK(cudaMemsetAsync(A.gf, 0, 3 * N * sizeof(double), st));
+    if (body) CK(cudaMemsetAsync(A.geta, 0, N * sizeof(double), st));
+    else A.geta = nullptr;
     CK(cudaMemsetAsync(A.gval, 0, 18 * sizeof(double), st));
     if (int rc = prepare_steps(ctx, std::max(K, M))) return rc;
     auto save_state = [&](double* dst) -> int {
@@ -2175,10 +2250,11 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         if (s % M == 0)
             if (int rc = save_state(ckpt + (size_t)(s / M) * 4 * N)) return rc;
         if (s >= last0) {
-            double* dst = blk + (size_t)(s - last0) * 3 * N;
+            double* dst = blk + (size_t)(s - last0) * bw * N;
             CK(cudaMemcpyAsync(dst, ctx->u, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(dst + N, ctx->v, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(dst + 2 * N, ctx->w, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if (body) CK(cudaMemcpyAsync(dst + 3 * N, ctx->p, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
         }
         if (int rc = launch_step(ctx)) return rc;
         k_pack_guards<<<148, 256, 0, st>>>(g, ctx->FXz, ctx->FYz, ctx->FXy, ctx->FYy, guards + (size_t)s * G);
@@ -2220,10 +2296,11 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         CK(cudaMemsetAsync(&ctx->ctl->step, 0, sizeof(int), st));
         CK(cudaEventRecord(ev.c, st));
         for (int m = 0; m < s1 - s0 && b < nck - 1; ++m) {
-            double* dst = blk + (size_t)m * 3 * N;
+            double* dst = blk + (size_t)m * bw * N;
             CK(cudaMemcpyAsync(dst, ctx->u, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(dst + N, ctx->v, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             CK(cudaMemcpyAsync(dst + 2 * N, ctx->w, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            if (body) CK(cudaMemcpyAsync(dst + 3 * N, ctx->p, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             if (m + 1 < s1 - s0) {
                 if (int rc = launch_step(ctx)) return rc;
                 ++recomputed;
@@ -2235,9 +2312,15 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         CK(cudaEventElapsedTime(&bms, ev.c, ev.d));
         rms += bms;
         for (int n = s1 - 1; n >= s0; --n) {
-            const double* sb = blk + (size_t)(n - s0) * 3 * N;
-            if (int rc = adjoint_step<Tc>(ctx, A, sb, sb + N, sb + 2 * N, guards + (size_t)n * G, scaleD, scaleL,
-                                          zrel, itmax, omega, &sweeps, &unconv))
+            const double* sb = blk + (size_t)(n - s0) * bw * N;
+            // the pressure after step n: before step n+1 (this block, the next checkpoint, or the end)
+            const double* pn = !body ? nullptr
+                               : n + 1 < s1 ? blk + (size_t)(n + 1 - s0) * bw * N + 3 * N
+                               : n + 1 < K  ? ckpt + (size_t)(b + 1) * 4 * N + 3 * N
+                                            : fin + 3 * N;
+            if (int rc = adjoint_step<Tc>(ctx, A, sb, sb + N, sb + 2 * N, body ? sb + 3 * N : nullptr, pn,
+                                          guards + (size_t)n * G, scaleD, scaleL, zrel, itmax, omega, &sweeps,
+                                          &unconv))
                 return rc;
         }
     }
@@ -2263,6 +2346,20 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(gout[c], ctx->outbuf, n * sizeof(double), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
+    }
+    // dJ/dAOA through the body: sum over the cells of dJ/dETA dETA/dAOA
+    res->dJ_daoa_body = 0.0;
+    if (body) {
+        const size_t cells = (size_t)g.ny * g.nz;
+        k_colsum_i<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, st>>>(g, A.geta, A.etacol);
+        CK(cudaGetLastError());
+        std::vector<double> col(cells), de(cells);
+        CK(cudaMemcpyAsync(col.data(), A.etacol, cells * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(de.data(), ctx->deta_daoa, cells * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        double sum = 0.0;
+        for (size_t q = 0; q < cells; ++q) sum += col[q] * de[q];
+        res->dJ_daoa_body = sum;
     }
     // the state after the K steps, as the forward pass left it
     if (int rc = load_state(fin)) return rc;

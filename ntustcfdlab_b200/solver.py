@@ -202,6 +202,13 @@ class Solver:
                                                       zc, yc, ctypes.byref(ties)))
         return ties.value
 
+    def build_mask_smooth(self, az, ay, aoa_deg, zc, yc, width):
+        """The body of build_mask_polygon blurred over +-width (a C1 ramp of the
+        signed distance); the adjoint then also returns dJ_daoa_body."""
+        az = np.ascontiguousarray(az, dtype=np.float64)
+        ay = np.ascontiguousarray(ay, dtype=np.float64)
+        self._check(self.lib.ntcfd_build_mask_smooth(self.h, dptr(az), dptr(ay), len(az), aoa_deg, zc, yc, width))
+
     def build_mask_cylinder(self, zc, yc, r):
         """DFIB_Cylinder (DFIB.f90:74-145) on the device."""
         self._check(self.lib.ntcfd_build_mask_cylinder(self.h, zc, yc, r))
@@ -298,7 +305,8 @@ class Solver:
         values that hold U cos(theta), U sin(theta).  initial_bc applies the
         boundary conditions to the state first and differentiates through
         them (otherwise the state, ghosts included, is fixed).  Returns a dict with J,
-        dJ_dbc (6x3), dJ_dU, dJ_dtheta, dJ_df (3 arrays or None), the step
+        dJ_dbc (6x3), dJ_dU, dJ_dtheta, dJ_daoa_body (per radian, with the mask
+        of build_mask_smooth), dJ_df (3 arrays or None), the step
         records and the timings; the solver is left after the nsteps steps."""
         spec = abi.NtcfdAdjSpec()
         spec.nsteps, spec.checkpoint_every = nsteps, checkpoint_every
@@ -321,7 +329,7 @@ class Solver:
         return {
             "J": res.J,
             "dJ_dbc": np.array([[res.dJ_dbc[w][c] for c in range(3)] for w in range(6)]),
-            "dJ_dU": res.dJ_dU, "dJ_dtheta": res.dJ_dtheta,
+            "dJ_dU": res.dJ_dU, "dJ_dtheta": res.dJ_dtheta, "dJ_daoa_body": res.dJ_daoa_body,
             "dJ_df": grads if force_grad else None,
             "forward_ms": res.forward_ms, "total_ms": res.total_ms,
             "recompute_ms": res.recompute_ms, "solve_ms": res.solve_ms,

@@ -220,3 +220,56 @@ def test_torch_gradcheck_on_inflow():
     U = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
     th = torch.tensor(math.radians(5.0), dtype=torch.float64, requires_grad=True)
     assert torch.autograd.gradcheck(f, (U, th), eps=H, atol=1e-7, rtol=FD_RTOL)
+
+
+# ---------------------------------------------------------------- body angle
+AOA_B, ZC_B, YC_B, WIDTH = 8.0, 2.3, 3.1, 0.3
+
+
+def _smooth_solver(case, state, aoa):
+    from ntustcfdlab_b200.solver import naca4_polygon
+    z, y = naca4_polygon(0.12, 64)
+    s = Solver(case.params, case.grid)
+    s.set_state(*state)
+    s.build_mask_smooth(z, y, aoa, ZC_B, YC_B, WIDTH)
+    return s
+
+
+def _smooth_objective(case, state, aoa):
+    s = _smooth_solver(case, state, aoa)
+    try:
+        info, rc = s.step(K)
+        assert rc == 0
+        return sum(W_DRAG * i.cDrag + W_LIFT * i.cLift for i in info) / K
+    finally:
+        s.close()
+
+
+def test_body_angle_gradient_matches_central_differences():
+    """dJ/dAOA through the rotating body (the smoothed NACA0012 mask of
+    ntcfd_build_mask_smooth), against central differences of complete K-step
+    runs with the same mask at AOA +- h; beside it the freestream-angle
+    gradient of the same run, a different quantity."""
+    case = small_case()
+    state = initial_state(case)
+    s = _smooth_solver(case, state, AOA_B)
+    try:
+        eta = s.get_mask()
+        assert eta.min() >= 0.0 and eta.max() == 1.0
+        assert np.count_nonzero((eta > 0) & (eta < 1)) > 50          # the blurred band
+        r = s.adjoint(K, 2, w_drag=W_DRAG, w_lift=W_LIFT, adj_zeta=1e-12, inflow=("Back", 2, 1))
+        assert r["status"] == 0
+    finally:
+        s.close()
+    assert r["J"] == _smooth_objective(case, state, AOA_B)
+    h = 1e-4                                                         # degrees
+    g = (_smooth_objective(case, state, AOA_B + h) - _smooth_objective(case, state, AOA_B - h)) / (2 * h)
+    g *= 180.0 / math.pi                                             # per radian
+    assert abs(g) > 1e-3
+    assert abs(r["dJ_daoa_body"] - g) <= FD_RTOL * abs(g), (r["dJ_daoa_body"], g)
+    assert r["dJ_daoa_body"] != r["dJ_dtheta"]
+
+
+def test_body_angle_gradient_is_zero_without_the_smoothed_mask(base):
+    case, state, force, r = base
+    assert r["dJ_daoa_body"] == 0.0
