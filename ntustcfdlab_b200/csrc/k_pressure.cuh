@@ -240,11 +240,15 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
                                               const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
                                               const Tc* __restrict__ rdOwn, int colour, double omega,
                                               const Ctl* ctl, int sub, int itmax, int cycle_len,
-                                              int guard, unsigned long long* slots) {
+                                              int guard, unsigned long long* slots, int first_mode) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
         if (ik + sub >= itmax || inner + sub >= cycle_len) return;
     }
+    // first sweep of a cycle (first_mode): e = 0 everywhere before it, so the red
+    // half reads no e at all and the black half no e of its own
+    const bool first = first_mode && ctl->inner + sub == 0;
+    const bool zN = first && colour == 0;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k0 = blockIdx.z * KPT + 1;
@@ -267,14 +271,14 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
         const int rr = ok[kk] ? r : 1;
         const int qq = (ok[kk] ? t + 2 - r : 1) + rowj + zs * (k + 1);
         q[kk] = qq;
-        nE[kk] = eOth[qq + rr];
-        nW[kk] = eOth[qq - 1 + rr];
-        nN[kk] = eOth[qq + ys];
-        nS[kk] = eOth[qq - ys];
-        nF[kk] = eOth[qq + zs];
-        nB[kk] = eOth[qq - zs];
+        nE[kk] = zN ? Tc(0) : eOth[qq + rr];
+        nW[kk] = zN ? Tc(0) : eOth[qq - 1 + rr];
+        nN[kk] = zN ? Tc(0) : eOth[qq + ys];
+        nS[kk] = zN ? Tc(0) : eOth[qq - ys];
+        nF[kk] = zN ? Tc(0) : eOth[qq + zs];
+        nB[kk] = zN ? Tc(0) : eOth[qq - zs];
         dd[kk] = dOwn[qq];
-        e0[kk] = eOwn[qq];
+        e0[kk] = first ? Tc(0) : eOwn[qq];
         rd[kk] = rdOwn[qq];
     }
     const Tc cN = sc.cN[jj], cS = sc.cS[jj];
@@ -306,15 +310,18 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
 // sweep budget (itmax, cycle length) is used up.  The block's max |change|
 // goes to slot sub*kSpread + (block index mod kSpread).
 template <class Tc, int NT>
-__global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
+__global__ void __launch_bounds__(NT, 5) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
                                               const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
                                               const Tc* __restrict__ rdOwn, int colour, double omega,
                                               const Ctl* ctl, int sub, int itmax, int cycle_len,
-                                              int guard, unsigned long long* slots) {
+                                              int guard, unsigned long long* slots, int first_mode) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
         if (ik + sub >= itmax || inner + sub >= cycle_len) return;
     }
+    // first sweep of a cycle (first_mode): as k_sweep_cols
+    const bool first = first_mode && ctl->inner + sub == 0;
+    const bool zN = first && colour == 0;
     using B = decltype(abs_bits(Tc(0)));
     const int lane = threadIdx.x & 31;
     const int nrow = g.ny * g.nz;
@@ -350,11 +357,14 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
             const int mA = tA + 2 - r, mB = okB ? tB + 2 - r : mA;
             const int iB = okB ? iB0 : iA;
             const Tc eA = sc.cE[iA], wA = sc.cW[iA], eB = sc.cE[iB], wB = sc.cW[iB];
-            const Tc nEA = oC[mA + r], nWA = oC[mA - 1 + r], nNA = oN[mA], nSA = oS[mA], nFA = oF[mA],
-                     nBA = oB[mA];
-            const Tc nEB = oC[mB + r], nWB = oC[mB - 1 + r], nNB = oN[mB], nSB = oS[mB], nFB = oF[mB],
-                     nBB = oB[mB];
-            const Tc dA = dR[mA], dB_ = dR[mB], e0A = eR[mA], e0B = eR[mB];
+            Tc nEA = Tc(0), nWA = Tc(0), nNA = Tc(0), nSA = Tc(0), nFA = Tc(0), nBA = Tc(0);
+            Tc nEB = Tc(0), nWB = Tc(0), nNB = Tc(0), nSB = Tc(0), nFB = Tc(0), nBB = Tc(0);
+            if (!zN) {
+                nEA = oC[mA + r]; nWA = oC[mA - 1 + r]; nNA = oN[mA]; nSA = oS[mA]; nFA = oF[mA]; nBA = oB[mA];
+                nEB = oC[mB + r]; nWB = oC[mB - 1 + r]; nNB = oN[mB]; nSB = oS[mB]; nFB = oF[mB]; nBB = oB[mB];
+            }
+            const Tc dA = dR[mA], dB_ = dR[mB];
+            const Tc e0A = first ? Tc(0) : eR[mA], e0B = first ? Tc(0) : eR[mB];
             const Tc rdA = kFormRd ? rcp_rn(((eA + wA) + sNS) + sFB) : rR[mA];
             const Tc rdB = kFormRd ? rcp_rn(((eB + wB) + sNS) + sFB) : rR[mB];
             Tc e1A, e1B;
@@ -373,15 +383,67 @@ __global__ void __launch_bounds__(NT) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* _
     block_max_bits<NT>(ch, &slots[sub * kSpread + (blockIdx.x & (kSpread - 1))]);
 }
 
-// Launch shape of k_sweep_rows: NT threads, warps striding over the rows, at
-// most kSweepRowBlocks blocks per SM (about the resident count), so a block's
-// max reduction and start-up are paid once for many rows.
-constexpr int kSweepRowBlocks = 6;
-inline dim3 sweep_grid(const Geom& g, int nt, int sms) {
+// Launch shape of the row kernels (k_sweep_rows, k_defect_rows): NT threads,
+// warps striding over the rows, at most `resident` blocks (the count the SMs
+// hold at once), so that every block runs from the start and a block's max
+// reduction and start-up are paid once for many rows.
+inline dim3 sweep_grid(const Geom& g, int nt, int resident) {
     const long long rows = (long long)g.ny * g.nz;
     const long long need = (rows + nt / 32 - 1) / (nt / 32);
-    const long long cap = (long long)kSweepRowBlocks * (sms > 0 ? sms : 1);
+    const long long cap = resident > 0 ? resident : 1;
     return dim3((unsigned)(need < cap ? need : cap));
+}
+
+// The restart of a correction cycle of the streaming path in row form (the
+// layout of k_sweep_rows): a warp per row (j,k), both colours, a cell per lane
+// and step.  The first cycle of a solve (ctl->cycles == 0) takes d from p:
+// defect_value, the FP64 defect of p; later cycles update it from the cycle's
+// e: defect_update, the same values k_defect forms.  e stays in place: the next
+// sweep, a cycle's first, reads it as zero (first_mode).  Block 0 starts the
+// cycle: inner sweep count and the inner loop's condition.
+template <class Tc, int NT>
+__global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> sc, SorCoef<Tc> st, const double* p,
+                                                    const double* b, Tc* dR, Tc* dB, const Tc* eR, const Tc* eB,
+                                                    Ctl* ctl, cudaGraphConditionalHandle inner, int in_graph) {
+    const bool incr = ctl->cycles > 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ctl->inner = 0;
+        if (in_graph) cudaGraphSetConditional(inner, 1u);
+    }
+    const int lane = threadIdx.x & 31;
+    const int nrow = g.ny * g.nz;
+    const int nwarp = (int)gridDim.x * (NT / 32);
+    const int ys = g.mxp;
+    const long long zs = g.mz;
+    const int half = (g.nx + 1) / 2;
+    for (int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5); row < nrow; row += nwarp) {
+        const int j = row % g.ny + 1, k = row / g.ny + 1;
+        const long long rb = (long long)ys * (j + 1) + zs * (k + 1);
+        const double cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
+        const Tc sNS = st.cN[j] + st.cS[j], sFB = st.cF[k] + st.cB[k];
+        for (int colour = 0; colour < 2; ++colour) {
+            const int r = ((j + k) ^ colour) & 1;
+            const Tc* __restrict__ O = (colour ? eR : eB) + rb;
+            const Tc* __restrict__ E = (colour ? eB : eR) + rb;
+            Tc* __restrict__ D = (colour ? dB : dR) + rb;
+            for (int t = lane; t < half; t += 32) {
+                const int i = 2 * t + 2 - r;
+                if (i > g.nx) break;
+                const int m = t + 2 - r;
+                double dn;
+                if (incr) {
+                    const Tc rd = rcp_rn(((st.cE[i] + st.cW[i]) + sNS) + sFB);
+                    dn = defect_update(sc.cE[i], O[m + r], sc.cW[i], O[m - 1 + r], cN, O[m + ys], cS, O[m - ys],
+                                       cF, O[m + zs], cB, O[m - zs], rd, D[m], E[m]);
+                } else {
+                    const long long c = nat(g, i, j, k);
+                    dn = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], cN, p[c + g.px], cS, p[c - g.px], cF,
+                                      p[c + g.pz], cB, p[c - g.pz], rdiag_of(sc, i, j, k), b[c], p[c]);
+                }
+                D[m] = (Tc)dn;
+            }
+        }
+    }
 }
 
 // One warp: the max over the kSpread slots of that sweep is its max|change|.

@@ -65,7 +65,7 @@ template <>
 struct Sweep<float> {
     static constexpr auto fn = k_sweep_rows<float, kSweepNT>;
     static dim3 block() { return dim3(kSweepNT); }
-    static dim3 grid(const Geom& g, int sms) { return sweep_grid(g, kSweepNT, sms); }
+    static dim3 grid(const Geom& g, int resident) { return sweep_grid(g, kSweepNT, resident); }
 };
 
 struct DevTabs {
@@ -115,6 +115,8 @@ struct ntcfd_ctx {
     size_t res_smem = 0;
     int res_grid = 0;
     int sm_count = 0;
+    int row_resident = 1;                   // resident blocks of k_sweep_rows (its grid cap)
+    int defect_resident = 1;                // and of k_defect_rows
     size_t smem_optin = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -494,12 +496,10 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
         cudaGraphNode_t m;
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
         // the defect of p (first cycle) or its update from the last cycle's e (later
-        // cycles, as the resident kernel restarts), then e = 0
-        GK(add_kernel(&m, outer, od, k_defect<Tc>, g3, b3, g, ctx->scd, (const double*)ctx->p,
-                      (const double*)ctx->b, dR, dB, eR, eB, (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl,
-                      hin, 1, (unsigned long long*)nullptr, (unsigned int*)nullptr, 0, 1));
-        od = {m};
-        GK(add_kernel(&m, outer, od, k_clear_e<Tc>, g3, b3, g, eR, eB));
+        // cycles, as the resident kernel restarts); the cycle's first sweep reads e as 0
+        GK(add_kernel(&m, outer, od, k_defect_rows<Tc, kSweepNT>, sweep_grid(g, kSweepNT, ctx->defect_resident),
+                      dim3(kSweepNT), g, ctx->scd, sor_coef<Tc>(ctx), (const double*)ctx->p,
+                      (const double*)ctx->b, dR, dB, (const Tc*)eR, (const Tc*)eB, ctx->ctl, hin, 1));
         od = {m};
         cudaGraph_t inner;
         GK(add_while(&m, outer, od, hin, &inner));
@@ -508,18 +508,18 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
             std::vector<cudaGraphNode_t> id;
             cudaGraphNode_t s;
             const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->row_resident);
             const Ctl* cctl = ctx->ctl;
             for (int sub = 0; sub < ctx->csweeps; ++sub) {
                 GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eR, (const Tc*)eB, (const Tc*)dR, (const Tc*)ctx->rdR, 0, P.omega, cctl,
                               sub, P.itmax,
-                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, 1));
                 id = {s};
                 GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eB, (const Tc*)eR, (const Tc*)dB, (const Tc*)ctx->rdB, 1, P.omega, cctl,
                               sub, P.itmax,
-                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots));
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, 1));
                 id = {s};
             }
             GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(32), ctx->ctl, ctx->slots,
@@ -668,18 +668,17 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
     const int big_guard = ctx->csweeps > 1 ? 1 : 0;
     while (more) {
         {
-            k_defect<Tc><<<g3, b3, 0, st>>>(g, ctx->scd, p, b, dR, dB, eR, eB, (const Tc*)ctx->rdR,
-                                            (const Tc*)ctx->rdB, ctx->ctl, 0, 0, nullptr, nullptr, 0, 1);
-            k_clear_e<Tc><<<g3, b3, 0, st>>>(g, eR, eB);
-            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
+            k_defect_rows<Tc, kSweepNT><<<sweep_grid(g, kSweepNT, ctx->defect_resident), kSweepNT, 0, st>>>(
+                g, ctx->scd, sc, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0);
+            const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->row_resident);
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
                     Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots);
+                        ctx->cycle_len, big_guard, ctx->slots, 1);
                     Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots);
+                        ctx->cycle_len, big_guard, ctx->slots, 1);
                 }
                 k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
                                               zeta, 0, 0);
@@ -834,20 +833,26 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
          }, &out->rhs_ms, 1)))
         return rc;
     Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
+    // the defect the path's restarts use: k_defect (resident), k_defect_rows (streaming)
     if ((rc = timed([&] {
-             k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
-                                                      (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl, 0, 0,
-                                                      nullptr, nullptr, 0, 0);
+             if (ctx->resident)
+                 k_defect<Tc><<<g3, b3, 0, ctx->stream>>>(g, ctx->scd, ctx->p, ctx->b, dR, dB, eR, eB,
+                                                          (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl, 0, 0,
+                                                          nullptr, nullptr, 0, 0);
+             else
+                 k_defect_rows<Tc, kSweepNT><<<sweep_grid(g, kSweepNT, ctx->defect_resident), kSweepNT, 0,
+                                               ctx->stream>>>(g, ctx->scd, sor_coef<Tc>(ctx), ctx->p, ctx->b, dR,
+                                                              dB, eR, eB, ctx->ctl, 0, 0);
          }, &out->defect_ms, 1)))
         return rc;
     const SorCoef<Tc> sc = sor_coef<Tc>(ctx);
-    const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->sm_count);
+    const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->row_resident);
     const int big = 1 << 30;
     if ((rc = timed([&] {
              Sweep<Tc>::fn<<<gs, bs, 0, ctx->stream>>>(
-                 g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
+                 g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots, 0);
              Sweep<Tc>::fn<<<gs, bs, 0, ctx->stream>>>(
-                 g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots);
+                 g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, P.omega, ctx->ctl, 0, big, big, 0, ctx->slots, 0);
          }, &out->sweep_ms, 2)))
         return rc;
     // the resident kernel: one launch of `nsw` sweeps (zeta = 0, one cycle) on a scratch
@@ -1006,6 +1011,16 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
         ctx->sm_count = v;
         CK(cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, P.device));
         ctx->smem_optin = (size_t)v;
+        // blocks of the row kernels the SMs hold at once (their grids stop there)
+        int a = 1, b = 1;
+        if (P.precision == NTCFD_MIXED) {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_sweep_rows<float, kSweepNT>, kSweepNT, 0));
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_defect_rows<float, kSweepNT>, kSweepNT, 0));
+        } else {
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_defect_rows<double, kSweepNT>, kSweepNT, 0));
+        }
+        ctx->row_resident = std::max(1, a) * ctx->sm_count;
+        ctx->defect_resident = std::max(1, b) * ctx->sm_count;
     }
     if ((rc = dalloc(ctx, &ctx->coordbuf, (size_t)(P.ny + 5) + (P.nz + 5) + 8))) return rc;
     ctx->coordY = ctx->coordbuf + 1;                  // Y[j] valid for j = -1..ny+3
@@ -1584,10 +1599,10 @@ int ntcfd_slab_stage(ntcfd_ctx* ctx, int stage, int colour) {
             break;
         case NTCFD_STAGE_HALFSWEEP: {   // colour 0: (i+j+k) even in the slab's own k; e of the other colour
             if (colour != 0 && colour != 1) return fail(ctx, NTCFD_EINVAL, "colour must be 0 or 1");
-            const dim3 bs = Sweep<double>::block(), gs = Sweep<double>::grid(g, ctx->sm_count);
+            const dim3 bs = Sweep<double>::block(), gs = Sweep<double>::grid(g, ctx->row_resident);
             Sweep<double>::fn<<<gs, bs, 0, st>>>(g, ctx->scd, colour ? eB : eR, colour ? eR : eB,
                                                  colour ? dB : dR, (const double*)(colour ? ctx->rdB : ctx->rdR),
-                                                 colour, P.omega, ctx->ctl, 0, P.itmax, P.itmax, 0, ctx->slots);
+                                                 colour, P.omega, ctx->ctl, 0, P.itmax, P.itmax, 0, ctx->slots, 0);
             break;
         }
         case NTCFD_STAGE_CORRECT:   // p += e

@@ -255,7 +255,8 @@ def test_body_angle_gradient_matches_central_differences():
     s = _smooth_solver(case, state, AOA_B)
     try:
         eta = s.get_mask()
-        assert eta.min() >= 0.0 and eta.max() == 1.0
+        # a 12 % thick section on 0.25 cells, blurred over +-0.3: no cell is fully inside
+        assert eta.min() >= 0.0 and 0.5 < eta.max() <= 1.0
         assert np.count_nonzero((eta > 0) & (eta < 1)) > 50          # the blurred band
         r = s.adjoint(K, 2, w_drag=W_DRAG, w_lift=W_LIFT, adj_zeta=1e-12, inflow=("Back", 2, 1))
         assert r["status"] == 0
