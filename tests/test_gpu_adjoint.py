@@ -240,7 +240,10 @@ def _smooth_objective(case, state, aoa):
     try:
         info, rc = s.step(K)
         assert rc == 0
-        return sum(W_DRAG * i.cDrag + W_LIFT * i.cLift for i in info) / K
+        J = 0.0                         # summed in the adjoint's order (sum() compensates)
+        for i in info:
+            J += W_DRAG * i.cDrag + W_LIFT * i.cLift
+        return J / K
     finally:
         s.close()
 
