@@ -234,21 +234,19 @@ __global__ void k_make_rd(Geom g, SorCoef<Tc> sc, Tc* rdR, Tc* rdB) {
 // 32-bit (a grid holds fewer than 2^31 cells per colour array).  With
 // guard = 1 (several sweeps per loop body) the sweep is skipped once the
 // sweep budget (itmax, cycle length) is used up.  The block's max |change|
-// goes to slot sub*kSpread + (block index mod kSpread).
+// goes to slot sub*kSpread + (block index mod kSpread).  It reads e as it is
+// (a cycle starts with k_clear_e); the first_mode argument of the row form is
+// not taken.
 template <class Tc, int NT, int KPT>
 __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
                                               const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
                                               const Tc* __restrict__ rdOwn, int colour, double omega,
                                               const Ctl* ctl, int sub, int itmax, int cycle_len,
-                                              int guard, unsigned long long* slots, int first_mode) {
+                                              int guard, unsigned long long* slots, int /*first_mode*/) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
         if (ik + sub >= itmax || inner + sub >= cycle_len) return;
     }
-    // first sweep of a cycle (first_mode): e = 0 everywhere before it, so the red
-    // half reads no e at all and the black half no e of its own
-    const bool first = first_mode && ctl->inner + sub == 0;
-    const bool zN = first && colour == 0;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k0 = blockIdx.z * KPT + 1;
@@ -271,14 +269,14 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
         const int rr = ok[kk] ? r : 1;
         const int qq = (ok[kk] ? t + 2 - r : 1) + rowj + zs * (k + 1);
         q[kk] = qq;
-        nE[kk] = zN ? Tc(0) : eOth[qq + rr];
-        nW[kk] = zN ? Tc(0) : eOth[qq - 1 + rr];
-        nN[kk] = zN ? Tc(0) : eOth[qq + ys];
-        nS[kk] = zN ? Tc(0) : eOth[qq - ys];
-        nF[kk] = zN ? Tc(0) : eOth[qq + zs];
-        nB[kk] = zN ? Tc(0) : eOth[qq - zs];
+        nE[kk] = eOth[qq + rr];
+        nW[kk] = eOth[qq - 1 + rr];
+        nN[kk] = eOth[qq + ys];
+        nS[kk] = eOth[qq - ys];
+        nF[kk] = eOth[qq + zs];
+        nB[kk] = eOth[qq - zs];
         dd[kk] = dOwn[qq];
-        e0[kk] = first ? Tc(0) : eOwn[qq];
+        e0[kk] = eOwn[qq];
         rd[kk] = rdOwn[qq];
     }
     const Tc cN = sc.cN[jj], cS = sc.cS[jj];
@@ -319,7 +317,8 @@ __global__ void __launch_bounds__(NT, 5) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc
         const int ik = ctl->ik, inner = ctl->inner;
         if (ik + sub >= itmax || inner + sub >= cycle_len) return;
     }
-    // first sweep of a cycle (first_mode): as k_sweep_cols
+    // first sweep of a cycle (first_mode): e = 0 everywhere before it, so the red
+    // half reads no e at all and the black half no e of its own
     const bool first = first_mode && ctl->inner + sub == 0;
     const bool zN = first && colour == 0;
     using B = decltype(abs_bits(Tc(0)));

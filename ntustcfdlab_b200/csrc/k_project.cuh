@@ -173,10 +173,7 @@ __device__ __forceinline__ double tangential(int kind, double val, double inner,
     }
 }
 
-__global__ void k_bc_x(Geom g, BcArgs a) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x - 1;
-    const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
-    if (j > g.ny + 2 || k > g.nz + 2) return;
+__device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, int k) {
     const int nx = g.nx;
     auto I = [&](int i) { return nat(g, i, j, k); };
     const bool inside = j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
@@ -244,10 +241,14 @@ __global__ void k_bc_x(Geom g, BcArgs a) {
     }
 }
 
-__global__ void k_bc_y(Geom g, BcArgs a) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+__global__ void k_bc_x(Geom g, BcArgs a) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x - 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
-    if (i > g.nx + 2 || k > g.nz + 2) return;
+    if (j > g.ny + 2 || k > g.nz + 2) return;
+    bc_x_at(g, a, j, k);
+}
+
+__device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, int k) {
     const int ny = g.ny;
     auto J = [&](int j) { return nat(g, i, j, k); };
     if (i >= 1 && i <= g.nx && k >= 1 && k <= g.nz) {
@@ -317,10 +318,14 @@ __global__ void k_bc_y(Geom g, BcArgs a) {
     }
 }
 
-__global__ void k_bc_z(Geom g, BcArgs a) {
+__global__ void k_bc_y(Geom g, BcArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
-    if (i > g.nx + 2 || j > g.ny + 2) return;
+    const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
+    if (i > g.nx + 2 || k > g.nz + 2) return;
+    bc_y_at(g, a, i, k);
+}
+
+__device__ __forceinline__ void bc_z_at(const Geom& g, const BcArgs& a, int i, int j) {
     const int nz = g.nz;
     auto K = [&](int k) { return nat(g, i, j, k); };
     if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
@@ -384,6 +389,13 @@ __global__ void k_bc_z(Geom g, BcArgs a) {
         if (a.bc[4][2] != BC_INTERFACE) { a.p[K(0)] = p1; a.p[K(-1)] = p1; }
         if (a.bc[5][2] != BC_INTERFACE) { a.p[K(nz + 1)] = pn; a.p[K(nz + 2)] = pn; }
     }
+}
+
+__global__ void k_bc_z(Geom g, BcArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
+    if (i > g.nx + 2 || j > g.ny + 2) return;
+    bc_z_at(g, a, i, j);
 }
 
 // ---------------------------------------------------------------- K8 ----

@@ -61,6 +61,11 @@ struct Sweep<double> {
                     (g.nz + kSweepKpt - 1) / kSweepKpt);
     }
 };
+// The row sweep (FP32) takes a cycle's first sweep with e read as zero; the
+// column sweep (FP64) runs after k_clear_e.
+template <class Tc>
+constexpr bool kRowSweep = sizeof(Tc) == 4;
+
 template <>
 struct Sweep<float> {
     static constexpr auto fn = k_sweep_rows<float, kSweepNT>;
@@ -496,11 +501,16 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
         cudaGraphNode_t m;
         Tc *eR = (Tc*)ctx->eR, *eB = (Tc*)ctx->eB, *dR = (Tc*)ctx->dR, *dB = (Tc*)ctx->dB;
         // the defect of p (first cycle) or its update from the last cycle's e (later
-        // cycles, as the resident kernel restarts); the cycle's first sweep reads e as 0
+        // cycles, as the resident kernel restarts); the row sweep (FP32) reads e as 0 in
+        // a cycle's first sweep, the column sweep (FP64) after k_clear_e
         GK(add_kernel(&m, outer, od, k_defect_rows<Tc, kSweepNT>, sweep_grid(g, kSweepNT, ctx->defect_resident),
                       dim3(kSweepNT), g, ctx->scd, sor_coef<Tc>(ctx), (const double*)ctx->p,
                       (const double*)ctx->b, dR, dB, (const Tc*)eR, (const Tc*)eB, ctx->ctl, hin, 1));
         od = {m};
+        if (!kRowSweep<Tc>) {
+            GK(add_kernel(&m, outer, od, k_clear_e<Tc>, g3, b3, g, eR, eB));
+            od = {m};
+        }
         cudaGraph_t inner;
         GK(add_while(&m, outer, od, hin, &inner));
         od = {m};
@@ -514,12 +524,12 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
                 GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eR, (const Tc*)eB, (const Tc*)dR, (const Tc*)ctx->rdR, 0, P.omega, cctl,
                               sub, P.itmax,
-                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, 1));
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, kRowSweep<Tc> ? 1 : 0));
                 id = {s};
                 GK(add_kernel(&s, inner, id, Sweep<Tc>::fn, gs, bs, g, sc,
                               eB, (const Tc*)eR, (const Tc*)dB, (const Tc*)ctx->rdB, 1, P.omega, cctl,
                               sub, P.itmax,
-                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, 1));
+                              ctx->cycle_len, ctx->csweeps > 1 ? 1 : 0, ctx->slots, kRowSweep<Tc> ? 1 : 0));
                 id = {s};
             }
             GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(32), ctx->ctl, ctx->slots,
@@ -561,12 +571,13 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
         dep = {n};
     }
     // kernels of a step: predictor, rhs, project, force (2, with a mask), bc (3), step_end, + LES,
-    // + diagnostic; + sor_begin and 4 per cycle (streaming) or 2 per solve (resident)
+    // + diagnostic; + sor_begin and 3 per cycle (streaming FP32; 4 with the FP64 clear) or
+    // 2 per solve (resident)
     const int fixed = extra + 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
                       (ctx->resident ? 0 : 1);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->resident ? 2 : 4, ctx->resident ? 0 : 2 * ctx->csweeps + 1,
-                  ctx->mask_nonzero ? 1 : 0, P.lx));
+                  P.diag_divergence, fixed, ctx->resident ? 2 : (kRowSweep<Tc> ? 3 : 4),
+                  ctx->resident ? 0 : 2 * ctx->csweeps + 1, ctx->mask_nonzero ? 1 : 0, P.lx));
     return 0;
 }
 
@@ -670,15 +681,16 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
         {
             k_defect_rows<Tc, kSweepNT><<<sweep_grid(g, kSweepNT, ctx->defect_resident), kSweepNT, 0, st>>>(
                 g, ctx->scd, sc, p, b, dR, dB, eR, eB, ctx->ctl, 0, 0);
+            if (!kRowSweep<Tc>) k_clear_e<Tc><<<g3, b3, 0, st>>>(g, eR, eB);
             const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->row_resident);
             for (;;) {
                 for (int sub = 0; sub < ctx->csweeps; ++sub) {
                     Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots, 1);
+                        ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
                     Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
                         g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots, 1);
+                        ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
                 }
                 k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
                                               zeta, 0, 0);
@@ -728,8 +740,9 @@ int run_step_eager(ntcfd_ctx* ctx) {
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
     const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
                       (ctx->resident ? 0 : 1);
-    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed, ctx->resident ? 2 : 4,
-                                ctx->resident ? 0 : 2 * ctx->csweeps + 1, ctx->mask_nonzero ? 1 : 0, P.lx);
+    k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed,
+                                ctx->resident ? 2 : (kRowSweep<Tc> ? 3 : 4), ctx->resident ? 0 : 2 * ctx->csweeps + 1,
+                                ctx->mask_nonzero ? 1 : 0, P.lx);
     CK(cudaGetLastError());
     return 0;
 }

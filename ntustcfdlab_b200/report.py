@@ -206,7 +206,23 @@ def main():
     ap.add_argument("--out", default=None)
     ap.add_argument("--moving", type=int, default=0,
                     help="instead: per-step cost of a moving body on c3 over this many steps")
+    ap.add_argument("--kernel-times", default=None, metavar="CASE",
+                    help="instead: one mixed step of CASE from its initial state, then the "
+                         "standalone kernel times (ntcfd_time_kernels, 10 launches each)")
     args = ap.parse_args()
+    if args.kernel_times:
+        fn, _ = WINDOWS[args.kernel_times]
+        c = fn(precision=MIXED)
+        s = _solver(c)
+        try:
+            s.set_state(*_initial_state(c))
+            s.boundary_conditions()
+            s.step(1)
+            kt = s.time_kernels(10)
+        finally:
+            s.close()
+        print(json.dumps({"case": args.kernel_times, "kernel_ms": {k: round(v, 5) for k, v in kt.items()}}))
+        return
     if args.moving:
         r = moving_body_cost("c3", args.moving, log=lambda m: print(m, flush=True))
         print(json.dumps(r), flush=True)
