@@ -340,39 +340,34 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
 
     // Restart of a correction cycle: d of every cell of the brick becomes the FP64
     // defect of p + e (defect_update), from the tiles (both rings current); one warp
-    // per row, lanes along i, the lane's cE, cW in registers.
-    constexpr int DU = 4;   // cells per lane per row and i-chunk
+    // per row and colour, lanes along the colour's cells (consecutive m, so each
+    // shared-memory load of the warp reads one tile without bank conflicts).
     auto update_defect = [&]() {
-        for (int ic = 1; ic <= g.nx; ic += 32 * DU) {
-            double ce[DU], cw[DU];
-#pragma unroll
-            for (int u = 0; u < DU; ++u) {
-                const int i = min(ic + lane + 32 * u, g.nx);
-                ce[u] = g.cE[i];
-                cw[u] = g.cW[i];
-            }
-            for (int row = warp; row < nrows; row += NWARP) {
-                const int jl = row % nj + 1, kl = row / nj + 1;
-                const int j = j0 + jl - 1, k = k0 + kl - 1;
-                const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-                const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
-                const long long g0 = spl(g, 0, j, k);
-#pragma unroll
-                for (int u = 0; u < DU; ++u) {
-                    const int i = ic + lane + 32 * u;
-                    if (i > g.nx) continue;
-                    const bool red = ((i + j + k) & 1) == 0;
-                    const Tc* O = red ? S1 : S0;
-                    const Tc* Wt = red ? S0 : S1;
-                    const int m = (i + 2) >> 1;
-                    const Tc dv = CD ? (red ? D0 : D1)[dr + m] : (red ? dRg : dBg)[g0 + m];
-                    const Tc rv = CR ? (red ? R0 : R1)[dr + m] : (red ? rdRg : rdBg)[g0 + m];
-                    const double dn = defect_update(ce[u], O[sr + ((i + 3) >> 1)], cw[u], O[sr + ((i + 1) >> 1)], cN,
-                                                    O[sr + mx + m], cS, O[sr - mx + m], cF, O[sr + plane + m], cB,
-                                                    O[sr - plane + m], rv, dv, Wt[sr + m]);
-                    if (CD) (red ? D0 : D1)[dr + m] = (Tc)dn;
-                    else (red ? dRg : dBg)[g0 + m] = (Tc)dn;
-                }
+        const int half = (g.nx + 1) / 2;
+        for (int rc = warp; rc < 2 * nrows; rc += NWARP) {
+            const int row = rc >> 1, c = rc & 1;
+            const int jl = row % nj + 1, kl = row / nj + 1;
+            const int j = j0 + jl - 1, k = k0 + kl - 1;
+            const int r = ((j + k) ^ c) & 1;
+            const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
+            const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
+            const long long g0 = spl(g, 0, j, k);
+            const Tc* O = (c ? S0 : S1) + sr;         // the other colour's tile row
+            const Tc* Wt = (c ? S1 : S0) + sr;        // this colour's
+            Tc* Dt = (c ? D1 : D0) + dr;
+            const Tc* Rt = (c ? R1 : R0) + dr;
+            Tc* Dg = (c ? dBg : dRg) + g0;
+            const Tc* Rg = (c ? rdBg : rdRg) + g0;
+            for (int t = lane; t < half; t += 32) {
+                const int i = 2 * t + 2 - r;
+                if (i > g.nx) break;
+                const int m = t + 2 - r;
+                const Tc dv = CD ? Dt[m] : Dg[m];
+                const Tc rv = CR ? Rt[m] : Rg[m];
+                const double dn = defect_update(g.cE[i], O[m + r], g.cW[i], O[m - 1 + r], cN, O[mx + m], cS,
+                                                O[m - mx], cF, O[plane + m], cB, O[m - plane], rv, dv, Wt[m]);
+                if (CD) Dt[m] = (Tc)dn;
+                else Dg[m] = (Tc)dn;
             }
         }
     };
