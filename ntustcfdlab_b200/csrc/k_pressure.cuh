@@ -15,6 +15,8 @@
 // float and recovers p in double.
 #pragma once
 
+#include <type_traits>
+
 #include "ntcfd_common.cuh"
 
 namespace ntcfd {
@@ -300,85 +302,138 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
 // One half-sweep over colour `colour` (0 = red, (i+j+k) even), row form (used
 // for FP32 e).  A warp takes a row (j,k) at a time, striding over the rows
 // (rows j-fastest, so that neighbouring warps share their j+-1 neighbour
-// rows); the colour's cells of a row are contiguous in the
+// rows; the stride is split into its j and k parts once, so the next row
+// needs no division).  The colour's cells of a row are contiguous in the
 // colour-split arrays (m = t + 2 - r, r = ((j+k)^colour)&1, i = 2t + 2 - r),
-// so the row's base offsets are formed once and each lane updates two cells
-// per step (t and t + 32) with every load issued before its stores.  With
-// guard = 1 (several sweeps per loop body) the sweep is skipped once the
-// sweep budget (itmax, cycle length) is used up.  The block's max |change|
-// goes to slot sub*kSpread + (block index mod kSpread).
+// and lane t updates the cells t and t + 32 of each 64-cell chunk with every
+// load issued before its stores.  The row parity r is a template argument of
+// the chunk update, so each array is read through one lane address per row
+// with immediate offsets (east/west neighbour, second cell); rows of at most
+// 64 cells per colour keep their lanes' cE, cW of both parities in
+// registers.  A lane past the row's last cell reads inside the padded arrays
+// (a split row holds at least 2 + (nx+1)/2 entries, the tables nx + 5, and
+// the ghost rows and planes follow the interior ones), stores nothing and
+// leaves the change maximum alone.  With guard = 1 (several sweeps per loop
+// body) the sweep is skipped once the sweep budget (itmax, cycle length) is
+// used up.  The block's max |change| goes to slot
+// sub*kSpread + (block index mod kSpread).  In a cycle's first sweep
+// (first_mode) e is zero everywhere before it, so the red half reads no e at
+// all and the black half none of its own.  rdOwn is not read: the diagonal
+// is formed from the 1-D tables, the same bits as the rd arrays.
 template <class Tc, int NT>
-__global__ void __launch_bounds__(NT, 5) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
+__global__ void __launch_bounds__(NT, 4) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc* __restrict__ eOwn,
                                               const Tc* __restrict__ eOth, const Tc* __restrict__ dOwn,
-                                              const Tc* __restrict__ rdOwn, int colour, double omega,
+                                              const Tc* __restrict__ /*rdOwn*/, int colour, double omega,
                                               const Ctl* ctl, int sub, int itmax, int cycle_len,
                                               int guard, unsigned long long* slots, int first_mode) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
         if (ik + sub >= itmax || inner + sub >= cycle_len) return;
     }
-    // first sweep of a cycle (first_mode): e = 0 everywhere before it, so the red
-    // half reads no e at all and the black half no e of its own
     const bool first = first_mode && ctl->inner + sub == 0;
-    const bool zN = first && colour == 0;
     using B = decltype(abs_bits(Tc(0)));
     const int lane = threadIdx.x & 31;
-    const int nrow = g.ny * g.nz;
+    const int ny = g.ny, nrow = g.ny * g.nz;
     const int nwarp = (int)gridDim.x * (NT / 32);
+    const int w0 = blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+    const int nx = g.nx;
+    const int half = (nx + 1) / 2;
+    const int nown0 = nx / 2, nown1 = (nx + 1) / 2;
+    const long long ys = g.mxp, zs = g.mz;
+    const Tc om = (Tc)omega;
     B ch = B(0);   // max |change| as an order-preserving pattern (NaN stays on top)
-    for (int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5); row < nrow; row += nwarp) {
-        const int j = row % g.ny + 1, k = row / g.ny + 1;
-        const int r = ((j + k) ^ colour) & 1;
-        const int ys = g.mxp;
-        const long long zs = g.mz;
-        const long long rb = (long long)ys * (j + 1) + zs * (k + 1);   // colour-split row, m = 0
-        const Tc* __restrict__ oC = eOth + rb;
-        const Tc* __restrict__ oN = oC + ys;
-        const Tc* __restrict__ oS = oC - ys;
-        const Tc* __restrict__ oF = oC + zs;
-        const Tc* __restrict__ oB = oC - zs;
-        Tc* __restrict__ eR = eOwn + rb;
-        const Tc* __restrict__ dR = dOwn + rb;
-        const Tc* __restrict__ rR = rdOwn + rb;
-        const Tc cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
-        // FP32: rdiag formed here as rdiag_of forms it (the same bits as the rd array,
-        // one stream less); FP64: read
-        constexpr bool kFormRd = sizeof(Tc) == 4;
-        const Tc sNS = cN + cS, sFB = cF + cB;
-        const Tc om = (Tc)omega;
-        const int half = (g.nx + 1) / 2;
-        for (int tA = lane; tA < half; tA += 64) {
-            const int iA = 2 * tA + 2 - r;
-            if (iA > g.nx) break;
-            const int tB = tA + 32;
-            const int iB0 = 2 * tB + 2 - r;
-            const bool okB = tB < half && iB0 <= g.nx;
-            const int mA = tA + 2 - r, mB = okB ? tB + 2 - r : mA;
-            const int iB = okB ? iB0 : iA;
-            const Tc eA = sc.cE[iA], wA = sc.cW[iA], eB = sc.cE[iB], wB = sc.cW[iB];
-            Tc nEA = Tc(0), nWA = Tc(0), nNA = Tc(0), nSA = Tc(0), nFA = Tc(0), nBA = Tc(0);
-            Tc nEB = Tc(0), nWB = Tc(0), nNB = Tc(0), nSB = Tc(0), nFB = Tc(0), nBB = Tc(0);
-            if (!zN) {
-                nEA = oC[mA + r]; nWA = oC[mA - 1 + r]; nNA = oN[mA]; nSA = oS[mA]; nFA = oF[mA]; nBA = oB[mA];
-                nEB = oC[mB + r]; nWB = oC[mB - 1 + r]; nNB = oN[mB]; nSB = oS[mB]; nFB = oF[mB]; nBB = oB[mB];
+    // the lane's coefficients in a one-chunk row: cells t = lane + 32h of parity r at
+    // i = 2t + 2 - r (past the row's end: other table entries, never used)
+    Tc cEr[2][2], cWr[2][2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int i = min(2 * (lane + 32 * h) + 2 - r, nx + 2);
+            cEr[r][h] = sc.cE[i];
+            cWr[r][h] = sc.cW[i];
+        }
+
+    // cells t0 + lane and t0 + lane + 32 of a row of parity R; MD 0: a plain sweep,
+    // 1: own e zero before it, 2: e zero everywhere before it
+    auto chunk = [&](auto rr, auto md, const Tc* __restrict__ oC, Tc* __restrict__ eC,
+                     const Tc* __restrict__ dC, int t0, int nown, Tc eA, Tc wA, Tc eB, Tc wB, Tc cN, Tc cS,
+                     Tc cF, Tc cB, Tc sNS, Tc sFB) {
+        constexpr int R = decltype(rr)::value;
+        constexpr int MD = decltype(md)::value;
+        const int tA = t0 + lane;
+        const int m = tA + 2 - R;
+        const Tc* __restrict__ o = oC + m;
+        Tc nEA = Tc(0), nWA = Tc(0), nNA = Tc(0), nSA = Tc(0), nFA = Tc(0), nBA = Tc(0);
+        Tc nEB = Tc(0), nWB = Tc(0), nNB = Tc(0), nSB = Tc(0), nFB = Tc(0), nBB = Tc(0);
+        if (MD != 2) {
+            const Tc* __restrict__ oN = o + ys;
+            const Tc* __restrict__ oS = o - ys;
+            const Tc* __restrict__ oF = o + zs;
+            const Tc* __restrict__ oB = o - zs;
+            nEA = o[R]; nWA = o[R - 1]; nEB = o[32 + R]; nWB = o[31 + R];
+            nNA = oN[0]; nNB = oN[32]; nSA = oS[0]; nSB = oS[32];
+            nFA = oF[0]; nFB = oF[32]; nBA = oB[0]; nBB = oB[32];
+        }
+        const Tc* __restrict__ dd = dC + m;
+        Tc* __restrict__ ee = eC + m;
+        const Tc dA = dd[0], dB = dd[32];
+        const Tc e0A = MD ? Tc(0) : ee[0], e0B = MD ? Tc(0) : ee[32];
+        const Tc rdA = rcp_rn(((eA + wA) + sNS) + sFB);
+        const Tc rdB = rcp_rn(((eB + wB) + sNS) + sFB);
+        Tc e1A, e1B;
+        const Tc diffA = sor_update(eA, nEA, wA, nWA, cN, nNA, cS, nSA, cF, nFA, cB, nBA, rdA, dA, e0A, om, &e1A);
+        const Tc diffB = sor_update(eB, nEB, wB, nWB, cN, nNB, cS, nSB, cF, nFB, cB, nBB, rdB, dB, e0B, om, &e1B);
+        if (tA < nown) {
+            ee[0] = e1A;
+            const B db = abs_bits(diffA);
+            ch = db > ch ? db : ch;
+        }
+        if (tA + 32 < nown) {
+            ee[32] = e1B;
+            const B db = abs_bits(diffB);
+            ch = db > ch ? db : ch;
+        }
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    auto rows = [&](auto md) {
+        if (w0 >= nrow) return;
+        int j = w0 % ny + 1, k = w0 / ny + 1;
+        const int dj = nwarp % ny, dk = nwarp / ny;
+        for (int row = w0; row < nrow; row += nwarp) {
+            const int r = ((j + k) ^ colour) & 1;
+            const long long rb = ys * (j + 1) + zs * (k + 1);   // colour-split row, m = 0
+            const Tc* __restrict__ oC = eOth + rb;
+            Tc* __restrict__ eC = eOwn + rb;
+            const Tc* __restrict__ dC = dOwn + rb;
+            const Tc cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
+            const Tc sNS = cN + cS, sFB = cF + cB;
+            if (half <= 64) {
+                if (r == 0) chunk(I0{}, md, oC, eC, dC, 0, nown0, cEr[0][0], cWr[0][0], cEr[0][1], cWr[0][1], cN, cS,
+                                  cF, cB, sNS, sFB);
+                else chunk(I1{}, md, oC, eC, dC, 0, nown1, cEr[1][0], cWr[1][0], cEr[1][1], cWr[1][1], cN, cS, cF,
+                           cB, sNS, sFB);
+            } else {
+                const int nown = r ? nown1 : nown0;
+                for (int t0 = 0; t0 < nown; t0 += 64) {
+                    const int iA = min(2 * (t0 + lane) + 2 - r, nx + 2), iB = min(iA + 64, nx + 2);
+                    const Tc eA = sc.cE[iA], wA = sc.cW[iA], eB = sc.cE[iB], wB = sc.cW[iB];
+                    if (r == 0) chunk(I0{}, md, oC, eC, dC, t0, nown, eA, wA, eB, wB, cN, cS, cF, cB, sNS, sFB);
+                    else chunk(I1{}, md, oC, eC, dC, t0, nown, eA, wA, eB, wB, cN, cS, cF, cB, sNS, sFB);
+                }
             }
-            const Tc dA = dR[mA], dB_ = dR[mB];
-            const Tc e0A = first ? Tc(0) : eR[mA], e0B = first ? Tc(0) : eR[mB];
-            const Tc rdA = kFormRd ? rcp_rn(((eA + wA) + sNS) + sFB) : rR[mA];
-            const Tc rdB = kFormRd ? rcp_rn(((eB + wB) + sNS) + sFB) : rR[mB];
-            Tc e1A, e1B;
-            const Tc diffA = sor_update(eA, nEA, wA, nWA, cN, nNA, cS, nSA, cF, nFA, cB, nBA, rdA, dA, e0A, om, &e1A);
-            const Tc diffB = sor_update(eB, nEB, wB, nWB, cN, nNB, cS, nSB, cF, nFB, cB, nBB, rdB, dB_, e0B, om, &e1B);
-            eR[mA] = e1A;
-            const B dbA = abs_bits(diffA);
-            ch = dbA > ch ? dbA : ch;
-            if (okB) {
-                eR[mB] = e1B;
-                const B dbB = abs_bits(diffB);
-                ch = dbB > ch ? dbB : ch;
+            j += dj;
+            k += dk;
+            if (j > ny) {
+                j -= ny;
+                ++k;
             }
         }
-    }
+    };
+    if (!first) rows(std::integral_constant<int, 0>{});
+    else if (colour != 0) rows(std::integral_constant<int, 1>{});
+    else rows(std::integral_constant<int, 2>{});
     block_max_bits<NT>(ch, &slots[sub * kSpread + (blockIdx.x & (kSpread - 1))]);
 }
 
@@ -396,12 +451,14 @@ inline dim3 sweep_grid(const Geom& g, int nt, int resident) {
 // The restart of a correction cycle of the streaming path in row form (the
 // layout of k_sweep_rows): a warp per row (j,k), both colours, a cell per lane
 // and step.  The first cycle of a solve (ctl->cycles == 0) takes d from p:
-// defect_value, the FP64 defect of p; later cycles update it from the cycle's
-// e: defect_update, the same values k_defect forms.  e stays in place: the next
-// sweep, a cycle's first, reads it as zero (first_mode).  Block 0 starts the
-// cycle: inner sweep count and the inner loop's condition.
+// defect_value, the FP64 defect of p; later cycles update it from the last
+// cycle's e (defect_update, the same values k_defect forms) and add that e to
+// p in the same pass (p += e of a cycle: the sweeps never read p, and the last
+// cycle's e goes to p in k_correct_last after the cycle loop).  e stays in
+// place: the next sweep, a cycle's first, reads it as zero (first_mode).
+// Block 0 starts the cycle: inner sweep count and the inner loop's condition.
 template <class Tc, int NT>
-__global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> sc, SorCoef<Tc> st, const double* p,
+__global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> sc, SorCoef<Tc> st, double* p,
                                                     const double* b, Tc* dR, Tc* dB, const Tc* eR, const Tc* eB,
                                                     Ctl* ctl, cudaGraphConditionalHandle inner, int in_graph) {
     const bool incr = ctl->cycles > 0;
@@ -432,8 +489,12 @@ __global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> s
                 double dn;
                 if (incr) {
                     const Tc rd = rcp_rn(((st.cE[i] + st.cW[i]) + sNS) + sFB);
+                    const Tc ev = E[m];
+                    double* pc = p + nat(g, i, j, k);
+                    const double pv = *pc;
                     dn = defect_update(sc.cE[i], O[m + r], sc.cW[i], O[m - 1 + r], cN, O[m + ys], cS, O[m - ys],
-                                       cF, O[m + zs], cB, O[m - zs], rd, D[m], E[m]);
+                                       cF, O[m + zs], cB, O[m - zs], rd, D[m], ev);
+                    *pc = pv + (double)ev;
                 } else {
                     const long long c = nat(g, i, j, k);
                     dn = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], cN, p[c + g.px], cS, p[c - g.px], cF,
@@ -480,6 +541,20 @@ __global__ void k_sor_check(Ctl* ctl, unsigned long long* slots, int csweeps, in
 // p += e over the interior (natural <- colour-split).
 template <class Tc>
 __global__ void __launch_bounds__(256) k_correct(Geom g, double* p, const Tc* eR, const Tc* eB) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
+    if (i > g.nx || j > g.ny || k > g.nz) return;
+    const long long q = spl(g, (i + 2) >> 1, j, k);
+    const Tc e = (((i + j + k) & 1) == 0) ? eR[q] : eB[q];
+    p[nat(g, i, j, k)] += (double)e;
+}
+
+// The streaming solve's final p += e: the e of its last correction cycle
+// (k_defect_rows adds the e of every earlier cycle); nothing when no cycle ran.
+template <class Tc>
+__global__ void __launch_bounds__(256) k_correct_last(Geom g, double* p, const Tc* eR, const Tc* eB, const Ctl* ctl) {
+    if (ctl->cycles == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;

@@ -504,7 +504,7 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
         // cycles, as the resident kernel restarts); the row sweep (FP32) reads e as 0 in
         // a cycle's first sweep, the column sweep (FP64) after k_clear_e
         GK(add_kernel(&m, outer, od, k_defect_rows<Tc, kSweepNT>, sweep_grid(g, kSweepNT, ctx->defect_resident),
-                      dim3(kSweepNT), g, ctx->scd, sor_coef<Tc>(ctx), (const double*)ctx->p,
+                      dim3(kSweepNT), g, ctx->scd, sor_coef<Tc>(ctx), ctx->p,
                       (const double*)ctx->b, dR, dB, (const Tc*)eR, (const Tc*)eB, ctx->ctl, hin, 1));
         od = {m};
         if (!kRowSweep<Tc>) {
@@ -535,9 +535,11 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
             GK(add_kernel(&s, inner, id, k_sor_check, dim3(1), dim3(32), ctx->ctl, ctx->slots,
                           ctx->csweeps, P.itmax, ctx->cycle_len, P.zeta, hin, 1));
         }
-        GK(add_kernel(&m, outer, od, k_correct<Tc>, g3, b3, g, ctx->p, (const Tc*)eR, (const Tc*)eB));
-        od = {m};
         GK(add_kernel(&m, outer, od, k_outer_check, dim3(1), dim3(1), ctx->ctl, P.itmax, hout, 1));
+        // the last cycle's e (k_defect_rows adds the earlier ones)
+        GK(add_kernel(&n, G, dep, k_correct_last<Tc>, g3, b3, g, ctx->p, (const Tc*)eR, (const Tc*)eB,
+                      (const Ctl*)ctx->ctl));
+        dep = {n};
     }
     ProjArgs pj{ctx->u, ctx->v, ctx->w, ctx->us, ctx->vs, ctx->ws, ctx->p, ctx->eta, ctx->partZ,
                 ctx->partY, P.dt, P.u_solid[0], P.u_solid[1], P.u_solid[2], kProjKc};
@@ -571,12 +573,12 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
         dep = {n};
     }
     // kernels of a step: predictor, rhs, project, force (2, with a mask), bc (3), step_end, + LES,
-    // + diagnostic; + sor_begin and 3 per cycle (streaming FP32; 4 with the FP64 clear) or
-    // 2 per solve (resident)
+    // + diagnostic; + sor_begin, the final correction and 2 per cycle (streaming FP32; 3 with
+    // the FP64 clear) or 2 per solve (resident)
     const int fixed = extra + 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
-                      (ctx->resident ? 0 : 1);
+                      (ctx->resident ? 0 : 2);
     GK(add_kernel(&n, G, dep, k_step_end, dim3(1), dim3(1), ctx->ctl, ctx->rec, ctx->divslot,
-                  P.diag_divergence, fixed, ctx->resident ? 2 : (kRowSweep<Tc> ? 3 : 4),
+                  P.diag_divergence, fixed, ctx->resident ? 2 : (kRowSweep<Tc> ? 2 : 3),
                   ctx->resident ? 0 : 2 * ctx->csweeps + 1, ctx->mask_nonzero ? 1 : 0, P.lx));
     return 0;
 }
@@ -697,12 +699,13 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
                 if (int rc = read_ctl()) return rc;
                 if (h.pad_stop) break;
             }
-            k_correct<Tc><<<g3, b3, 0, st>>>(g, p, eR, eB);
         }
         k_outer_check<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
         if (int rc = read_ctl()) return rc;
         more = h.pad_more != 0;
     }
+    // the last cycle's e (k_defect_rows adds the earlier ones)
+    k_correct_last<Tc><<<g3, b3, 0, st>>>(g, p, eR, eB, ctx->ctl);
     CK(cudaGetLastError());
     return 0;
 }
@@ -739,9 +742,9 @@ int run_step_eager(ntcfd_ctx* ctx) {
     k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
     const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
-                      (ctx->resident ? 0 : 1);
+                      (ctx->resident ? 0 : 2);
     k_step_end<<<1, 1, 0, st>>>(ctx->ctl, ctx->rec, ctx->divslot, P.diag_divergence, fixed,
-                                ctx->resident ? 2 : (kRowSweep<Tc> ? 3 : 4), ctx->resident ? 0 : 2 * ctx->csweeps + 1,
+                                ctx->resident ? 2 : (kRowSweep<Tc> ? 2 : 3), ctx->resident ? 0 : 2 * ctx->csweeps + 1,
                                 ctx->mask_nonzero ? 1 : 0, P.lx);
     CK(cudaGetLastError());
     return 0;
@@ -853,8 +856,10 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
                                                           (const Tc*)ctx->rdR, (const Tc*)ctx->rdB, ctx->ctl, 0, 0,
                                                           nullptr, nullptr, 0, 0);
              else
+                 // on scratch (us is rewritten by the predictor every step): from a
+                 // cycle on, the restart also adds e to the p it is given
                  k_defect_rows<Tc, kSweepNT><<<sweep_grid(g, kSweepNT, ctx->defect_resident), kSweepNT, 0,
-                                               ctx->stream>>>(g, ctx->scd, sor_coef<Tc>(ctx), ctx->p, ctx->b, dR,
+                                               ctx->stream>>>(g, ctx->scd, sor_coef<Tc>(ctx), ctx->us, ctx->b, dR,
                                                               dB, eR, eB, ctx->ctl, 0, 0);
          }, &out->defect_ms, 1)))
         return rc;
