@@ -77,28 +77,35 @@ __device__ __forceinline__ double defect_value(double cE, double pe, double cW, 
     return sub_rn(fma_rn(rd, s, -bv), pc);
 }
 
+// FP64 reciprocal of a coefficient sum (positive and finite): the hardware's
+// approximate double reciprocal refined by two Newton-Raphson steps
+// x' = x + x (1 - s x), each of which squares the relative error.
+__device__ __forceinline__ double rdiag64(double s) {
+    double x;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(x) : "d"(s));
+    double r = fma_rn(-s, x, 1.0);
+    x = fma_rn(x, r, x);
+    r = fma_rn(-s, x, 1.0);
+    x = fma_rn(x, r, x);
+    return x;
+}
+
 // The FP64 defect of p + e from the defect d of p and the correction e of a
 // defect-correction cycle: since the operator is linear,
 //     d' = rdiag sum c (p+e)_nb - b' - (p+e) = d + rdiag sum_nb c_nb e_nb - e,
 // formed in FP64 with the FP64 coefficients from the cycle's (exact) Tc
-// values of e.  rdiag is the FP64 reciprocal of the coefficient sum, refined
-// from the sweeps' rd by two Newton steps.  Both SOR paths restart a cycle
-// with it.
+// values of e; rdiag is rdiag64 of the FP64 coefficient sum.  Both SOR paths
+// restart a cycle with it.
 template <class Tc>
 __device__ __forceinline__ double defect_update(double cE, Tc eE, double cW, Tc eW, double cN, Tc eN, double cS,
-                                                Tc eS, double cF, Tc eF, double cB, Tc eB, Tc rd, Tc d, Tc e) {
+                                                Tc eS, double cF, Tc eF, double cB, Tc eB, Tc d, Tc e) {
     double s = mul_rn(cE, (double)eE);
     s = fma_rn(cW, (double)eW, s);
     s = fma_rn(cN, (double)eN, s);
     s = fma_rn(cS, (double)eS, s);
     s = fma_rn(cF, (double)eF, s);
     s = fma_rn(cB, (double)eB, s);
-    const double sum = ((cE + cW) + (cN + cS)) + (cF + cB);
-    double x = (double)rd;
-    double r = fma_rn(-sum, x, 1.0);
-    x = fma_rn(x, r, x);
-    r = fma_rn(-sum, x, 1.0);
-    x = fma_rn(x, r, x);
+    const double x = rdiag64(((cE + cW) + (cN + cS)) + (cF + cB));
     return sub_rn(fma_rn(x, s, (double)d), (double)e);
 }
 
@@ -190,7 +197,7 @@ __global__ void __launch_bounds__(256) k_defect(Geom g, SorCoef<double> sc, cons
         const Tc dv = (red ? dR : dB)[q];
         const double dn = defect_update(sc.cE[i], O[r0 + ((i + 3) >> 1)], sc.cW[i], O[r0 + ((i + 1) >> 1)], sc.cN[j],
                                         O[q + g.mxp], sc.cS[j], O[q - g.mxp], sc.cF[k], O[q + g.mz], sc.cB[k],
-                                        O[q - g.mz], (red ? rdR : rdB)[q], dv, (red ? eR : eB)[q]);
+                                        O[q - g.mz], dv, (red ? eR : eB)[q]);
         (red ? dR : dB)[q] = (Tc)dn;
         return;
     }
@@ -449,16 +456,22 @@ inline dim3 sweep_grid(const Geom& g, int nt, int resident) {
 }
 
 // The restart of a correction cycle of the streaming path in row form (the
-// layout of k_sweep_rows): a warp per row (j,k), both colours, a cell per lane
-// and step.  The first cycle of a solve (ctl->cycles == 0) takes d from p:
-// defect_value, the FP64 defect of p; later cycles update it from the last
-// cycle's e (defect_update, the same values k_defect forms) and add that e to
-// p in the same pass (p += e of a cycle: the sweeps never read p, and the last
-// cycle's e goes to p in k_correct_last after the cycle loop).  e stays in
-// place: the next sweep, a cycle's first, reads it as zero (first_mode).
-// Block 0 starts the cycle: inner sweep count and the inner loop's condition.
+// layout of k_sweep_rows): a warp per row (j,k), both colours, rows stepped as
+// in k_sweep_rows.  The first cycle of a solve (ctl->cycles == 0) takes d from
+// p: defect_value, the FP64 defect of p, a cell per lane and step.  Later
+// cycles update it from the last cycle's e (defect_update, the same values
+// k_defect forms) and add that e to p in the same pass (p += e of a cycle:
+// the sweeps never read p, and the last cycle's e goes to p in k_correct_last
+// after the cycle loop); there lane t takes the cells t and t + 32 of each
+// 64-cell chunk of a colour, the row parity a template argument as in
+// k_sweep_rows, every load issued before the stores.  A lane past the row's
+// last cell reads inside the padded arrays (the natural row of p holds nx + 10
+// entries or more and ghost rows and planes follow the interior) and stores
+// nothing.  e stays in place: the next sweep, a cycle's first, reads it as
+// zero (first_mode).  Block 0 starts the cycle: inner sweep count and the
+// inner loop's condition.
 template <class Tc, int NT>
-__global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> sc, SorCoef<Tc> st, double* p,
+__global__ void __launch_bounds__(NT, 3) k_defect_rows(Geom g, SorCoef<double> sc, SorCoef<Tc> /*st*/, double* p,
                                                     const double* b, Tc* dR, Tc* dB, const Tc* eR, const Tc* eB,
                                                     Ctl* ctl, cudaGraphConditionalHandle inner, int in_graph) {
     const bool incr = ctl->cycles > 0;
@@ -467,41 +480,84 @@ __global__ void __launch_bounds__(NT, 4) k_defect_rows(Geom g, SorCoef<double> s
         if (in_graph) cudaGraphSetConditional(inner, 1u);
     }
     const int lane = threadIdx.x & 31;
-    const int nrow = g.ny * g.nz;
+    const int ny = g.ny, nrow = g.ny * g.nz;
     const int nwarp = (int)gridDim.x * (NT / 32);
-    const int ys = g.mxp;
-    const long long zs = g.mz;
-    const int half = (g.nx + 1) / 2;
-    for (int row = blockIdx.x * (NT / 32) + (threadIdx.x >> 5); row < nrow; row += nwarp) {
-        const int j = row % g.ny + 1, k = row / g.ny + 1;
-        const long long rb = (long long)ys * (j + 1) + zs * (k + 1);
+    const int w0 = blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+    if (w0 >= nrow) return;
+    const int nx = g.nx;
+    const int half = (nx + 1) / 2;
+    const int nown0 = nx / 2, nown1 = (nx + 1) / 2;
+    const long long ys = g.mxp, zs = g.mz;
+
+    // cells t0 + lane and t0 + lane + 32 of colour arrays O (other), E (own), D of a
+    // row of parity R whose natural row of p starts at pr (i = 0)
+    auto chunk = [&](auto rr, const Tc* __restrict__ O, const Tc* __restrict__ E, Tc* __restrict__ D,
+                     double* __restrict__ pr, int t0, int nown, double cN, double cS, double cF, double cB) {
+        constexpr int R = decltype(rr)::value;
+        const int tA = t0 + lane;
+        const int m = tA + 2 - R;
+        const int iA = 2 * tA + 2 - R;
+        const int iAc = min(iA, nx + 2), iBc = min(iA + 64, nx + 2);
+        const Tc* __restrict__ o = O + m;
+        const Tc* __restrict__ oN = o + ys;
+        const Tc* __restrict__ oS = o - ys;
+        const Tc* __restrict__ oF = o + zs;
+        const Tc* __restrict__ oB = o - zs;
+        const Tc nEA = o[R], nWA = o[R - 1], nEB = o[32 + R], nWB = o[31 + R];
+        const Tc nNA = oN[0], nNB = oN[32], nSA = oS[0], nSB = oS[32];
+        const Tc nFA = oF[0], nFB = oF[32], nBA = oB[0], nBB = oB[32];
+        const Tc dA = D[m], dB_ = D[m + 32], eA = E[m], eB_ = E[m + 32];
+        double* __restrict__ pp = pr + iA;
+        const double pA = pp[0], pB = pp[64];
+        const double cEA = sc.cE[iAc], cWA = sc.cW[iAc], cEB = sc.cE[iBc], cWB = sc.cW[iBc];
+        const double dnA = defect_update(cEA, nEA, cWA, nWA, cN, nNA, cS, nSA, cF, nFA, cB, nBA, dA, eA);
+        const double dnB = defect_update(cEB, nEB, cWB, nWB, cN, nNB, cS, nSB, cF, nFB, cB, nBB, dB_, eB_);
+        if (tA < nown) {
+            D[m] = (Tc)dnA;
+            pp[0] = pA + (double)eA;
+        }
+        if (tA + 32 < nown) {
+            D[m + 32] = (Tc)dnB;
+            pp[64] = pB + (double)eB_;
+        }
+    };
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    int j = w0 % ny + 1, k = w0 / ny + 1;
+    const int dj = nwarp % ny, dk = nwarp / ny;
+    for (int row = w0; row < nrow; row += nwarp) {
+        const long long rb = ys * (j + 1) + zs * (k + 1);
         const double cN = sc.cN[j], cS = sc.cS[j], cF = sc.cF[k], cB = sc.cB[k];
-        const Tc sNS = st.cN[j] + st.cS[j], sFB = st.cF[k] + st.cB[k];
         for (int colour = 0; colour < 2; ++colour) {
             const int r = ((j + k) ^ colour) & 1;
             const Tc* __restrict__ O = (colour ? eR : eB) + rb;
             const Tc* __restrict__ E = (colour ? eB : eR) + rb;
             Tc* __restrict__ D = (colour ? dB : dR) + rb;
-            for (int t = lane; t < half; t += 32) {
-                const int i = 2 * t + 2 - r;
-                if (i > g.nx) break;
-                const int m = t + 2 - r;
-                double dn;
-                if (incr) {
-                    const Tc rd = rcp_rn(((st.cE[i] + st.cW[i]) + sNS) + sFB);
-                    const Tc ev = E[m];
-                    double* pc = p + nat(g, i, j, k);
-                    const double pv = *pc;
-                    dn = defect_update(sc.cE[i], O[m + r], sc.cW[i], O[m - 1 + r], cN, O[m + ys], cS, O[m - ys],
-                                       cF, O[m + zs], cB, O[m - zs], rd, D[m], ev);
-                    *pc = pv + (double)ev;
-                } else {
-                    const long long c = nat(g, i, j, k);
-                    dn = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], cN, p[c + g.px], cS, p[c - g.px], cF,
-                                      p[c + g.pz], cB, p[c - g.pz], rdiag_of(sc, i, j, k), b[c], p[c]);
+            if (incr) {
+                double* __restrict__ pr = p + nat(g, 0, j, k);
+                const int nown = r ? nown1 : nown0;
+                for (int t0 = 0; t0 < nown; t0 += 64) {
+                    if (r == 0) chunk(I0{}, O, E, D, pr, t0, nown, cN, cS, cF, cB);
+                    else chunk(I1{}, O, E, D, pr, t0, nown, cN, cS, cF, cB);
                 }
-                D[m] = (Tc)dn;
+            } else {
+                for (int t = lane; t < half; t += 32) {
+                    const int i = 2 * t + 2 - r;
+                    if (i > nx) break;
+                    const int m = t + 2 - r;
+                    const long long c = nat(g, i, j, k);
+                    const double dn = defect_value(sc.cE[i], p[c + 1], sc.cW[i], p[c - 1], cN, p[c + g.px], cS,
+                                                   p[c - g.px], cF, p[c + g.pz], cB, p[c - g.pz],
+                                                   rdiag_of(sc, i, j, k), b[c], p[c]);
+                    D[m] = (Tc)dn;
+                }
             }
+        }
+        j += dj;
+        k += dk;
+        if (j > ny) {
+            j -= ny;
+            ++k;
         }
     }
 }

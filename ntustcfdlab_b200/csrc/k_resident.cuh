@@ -355,17 +355,14 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             const Tc* O = (c ? S0 : S1) + sr;         // the other colour's tile row
             const Tc* Wt = (c ? S1 : S0) + sr;        // this colour's
             Tc* Dt = (c ? D1 : D0) + dr;
-            const Tc* Rt = (c ? R1 : R0) + dr;
             Tc* Dg = (c ? dBg : dRg) + g0;
-            const Tc* Rg = (c ? rdBg : rdRg) + g0;
             for (int t = lane; t < half; t += 32) {
                 const int i = 2 * t + 2 - r;
                 if (i > g.nx) break;
                 const int m = t + 2 - r;
                 const Tc dv = CD ? Dt[m] : Dg[m];
-                const Tc rv = CR ? Rt[m] : Rg[m];
                 const double dn = defect_update(g.cE[i], O[m + r], g.cW[i], O[m - 1 + r], cN, O[mx + m], cS,
-                                                O[m - mx], cF, O[plane + m], cB, O[m - plane], rv, dv, Wt[m]);
+                                                O[m - mx], cF, O[plane + m], cB, O[m - plane], dv, Wt[m]);
                 if (CD) Dt[m] = (Tc)dn;
                 else Dg[m] = (Tc)dn;
             }
