@@ -217,6 +217,71 @@ __device__ __forceinline__ void grad_gauss(const Geom& g, const double* f, bool 
     out[0] = fact * d1; out[1] = fact * d2; out[2] = fact * d3;
 }
 
+// The seven storage positions that phi_read reads for Phi(i,j,k) and its
+// six neighbours under REF_ALIASED, as natural-layout indices (-1: outside
+// the halo array, read as 0).  Storage element `off` sits at (a, b, c) =
+// (off mod ax, (off / ax) mod ay, off / (ax ay)) of the (nx+4) x (ny+4) x
+// (nz+4) array; the centre's position takes one division pair, and the
+// neighbours at off +- 1, +- nx, +- nx*ny follow by adding the offset's own
+// radix digits with one carry per digit (nx < ax and nx*ny < ax*ay).  The
+// halo array holds fewer than 2^32 elements.
+struct AliasPos {
+    long long q[7];   // P0, E (+1), W (-1), N (+nx), S (-nx), F (+nx ny), B (-nx ny)
+};
+__device__ __forceinline__ AliasPos alias_positions(const Geom& g, int i, int j, int k) {
+    const unsigned ax = g.nx + 4, ay = g.ny + 4, cz = g.nz + 4;
+    const unsigned nxny = (unsigned)g.nx * g.ny;
+    const unsigned fa = nxny % ax, fb = nxny / ax;   // nx*ny = fb*ax + fa, fb < ay
+    const unsigned off = (unsigned)(i - 1) + (unsigned)(j - 1) * g.nx + (unsigned)(k - 1) * nxny;
+    const int a0 = (int)(off % ax);
+    const unsigned t = off / ax;
+    const int b0 = (int)(t % ay), c0 = (int)(t / ay);
+    auto at = [&](int a, int b, int c) -> long long {
+        return (c < 0 || c >= (int)cz) ? -1 : nat(g, a - 1, b - 1, c - 1);
+    };
+    auto plus = [&](int da, int db) {
+        int a = a0 + da, b = b0 + db, c = c0;
+        if (a >= (int)ax) { a -= ax; ++b; }
+        if (b >= (int)ay) { b -= ay; ++c; }
+        return at(a, b, c);
+    };
+    auto minus = [&](int da, int db) {
+        int a = a0 - da, b = b0 - db, c = c0;
+        if (a < 0) { a += ax; --b; }
+        if (b < 0) { b += ay; --c; }
+        return at(a, b, c);
+    };
+    AliasPos p;
+    p.q[0] = at(a0, b0, c0);
+    p.q[1] = plus(1, 0);
+    p.q[2] = minus(1, 0);
+    p.q[3] = plus(g.nx, 0);
+    p.q[4] = minus(g.nx, 0);
+    p.q[5] = plus((int)fa, (int)fb);
+    p.q[6] = minus((int)fa, (int)fb);
+    return p;
+}
+
+// grad_gauss with the REF_ALIASED reads at precomputed positions (the same
+// values phi_read returns, the same arithmetic).
+__device__ __forceinline__ void grad_gauss_at(const Geom& g, const double* f, const AliasPos& P, int i, int j,
+                                              int k, const double* Dxm, const double* Dym, const double* Dzm,
+                                              double out[3]) {
+    auto rd = [&](int n) { return P.q[n] < 0 ? 0.0 : __ldg(f + P.q[n]); };
+    const double P0 = rd(0);
+    const double fe = 0.5 * (rd(1) + P0);
+    const double fw = 0.5 * (rd(2) + P0);
+    const double fn = 0.5 * (rd(3) + P0);
+    const double fs = 0.5 * (rd(4) + P0);
+    const double ff = 0.5 * (rd(5) + P0);
+    const double fb = 0.5 * (rd(6) + P0);
+    const double d1 = fw * (-1) * (Dym[j] * Dzm[k]) + fe * (1) * (Dym[j] * Dzm[k]);
+    const double d2 = fs * (-1) * (Dxm[i] * Dzm[k]) + fn * (1) * (Dxm[i] * Dzm[k]);
+    const double d3 = fb * (-1) * (Dxm[i] * Dym[j]) + ff * (1) * (Dxm[i] * Dym[j]);
+    const double fact = 1.0 / (Dxm[i] * Dym[j] * Dzm[k]);
+    out[0] = fact * d1; out[1] = fact * d2; out[2] = fact * d3;
+}
+
 __global__ void __launch_bounds__(256) k_smagorinsky(Geom g, const double* u, const double* v,
                                                      const double* w, double* nut, double Cs,
                                                      int aliased) {
@@ -224,11 +289,17 @@ __global__ void __launch_bounds__(256) k_smagorinsky(Geom g, const double* u, co
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int k = blockIdx.z * blockDim.z + threadIdx.z + 1;
     if (i > g.nx || j > g.ny || k > g.nz) return;
-    const bool al = aliased != 0;
     double du[3], dv[3], dw[3];
-    grad_gauss(g, u, al, i, j, k, g.Dxs, g.iDy, g.iDz, du);
-    grad_gauss(g, v, al, i, j, k, g.iDx, g.Dys, g.iDz, dv);
-    grad_gauss(g, w, al, i, j, k, g.iDx, g.iDy, g.Dzs, dw);
+    if (aliased) {
+        const AliasPos P = alias_positions(g, i, j, k);
+        grad_gauss_at(g, u, P, i, j, k, g.Dxs, g.iDy, g.iDz, du);
+        grad_gauss_at(g, v, P, i, j, k, g.iDx, g.Dys, g.iDz, dv);
+        grad_gauss_at(g, w, P, i, j, k, g.iDx, g.iDy, g.Dzs, dw);
+    } else {
+        grad_gauss(g, u, false, i, j, k, g.Dxs, g.iDy, g.iDz, du);
+        grad_gauss(g, v, false, i, j, k, g.iDx, g.Dys, g.iDz, dv);
+        grad_gauss(g, w, false, i, j, k, g.iDx, g.iDy, g.Dzs, dw);
+    }
     double m = fabs(2 * (du[0] * du[0]) + 2 * (dv[1] * dv[1]) + 2 * (dw[2] * dw[2]) +
                     (du[1] + dv[0]) * (du[1] + dv[0]) + (du[2] + dw[0]) * (du[2] + dw[0]) +
                     (dv[2] + dw[1]) * (dv[2] + dw[1]));
