@@ -339,16 +339,21 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     };
 
     // Restart of a correction cycle: d of every cell of the brick becomes the FP64
-    // defect of p + e (defect_update), from the tiles (both rings current); one warp
-    // per row and colour, lanes along the colour's cells (consecutive m, so each
-    // shared-memory load of the warp reads one tile without bank conflicts).
+    // defect of p + e (defect_update), from the tiles (both rings current), and the
+    // cycle's e goes to p in the same pass (add_e_to_p takes only the last cycle's);
+    // one warp per row and colour, lane t takes the cells t and t + 32 of each
+    // 64-cell chunk (consecutive m: each shared-memory load of the warp reads one
+    // tile without bank conflicts), every load of both issued before the FP64
+    // arithmetic.  A lane past the row's last cell reads inside the shared
+    // allocation, the padded d and rd arrays and the natural p array (ghost rows
+    // and planes follow the brick's) and stores nothing.
     auto update_defect = [&]() {
-        const int half = (g.nx + 1) / 2;
         for (int rc = warp; rc < 2 * nrows; rc += NWARP) {
             const int row = rc >> 1, c = rc & 1;
             const int jl = row % nj + 1, kl = row / nj + 1;
             const int j = j0 + jl - 1, k = k0 + kl - 1;
             const int r = ((j + k) ^ c) & 1;
+            const int nown = r ? nown1 : nown0;
             const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
             const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
             const long long g0 = spl(g, 0, j, k);
@@ -356,15 +361,32 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
             const Tc* Wt = (c ? S1 : S0) + sr;        // this colour's
             Tc* Dt = (c ? D1 : D0) + dr;
             Tc* Dg = (c ? dBg : dRg) + g0;
-            for (int t = lane; t < half; t += 32) {
-                const int i = 2 * t + 2 - r;
-                if (i > g.nx) break;
-                const int m = t + 2 - r;
-                const Tc dv = CD ? Dt[m] : Dg[m];
-                const double dn = defect_update(g.cE[i], O[m + r], g.cW[i], O[m - 1 + r], cN, O[mx + m], cS,
-                                                O[m - mx], cF, O[plane + m], cB, O[m - plane], dv, Wt[m]);
-                if (CD) Dt[m] = (Tc)dn;
-                else Dg[m] = (Tc)dn;
+            double* pr = p + nat(g, 0, j, k);
+            for (int t0 = 0; t0 < nown; t0 += 64) {
+                const int tA = t0 + lane;
+                const int mA = tA + 2 - r, mB = mA + 32;
+                const int iA = 2 * tA + 2 - r;
+                const int iAc = min(iA, g.nx + 2), iBc = min(iA + 64, g.nx + 2);
+                const Tc oEA = O[mA + r], oWA = O[mA - 1 + r], oNA = O[mx + mA], oSA = O[mA - mx];
+                const Tc oFA = O[plane + mA], oBA = O[mA - plane];
+                const Tc oEB = O[mB + r], oWB = O[mB - 1 + r], oNB = O[mx + mB], oSB = O[mB - mx];
+                const Tc oFB = O[plane + mB], oBB = O[mB - plane];
+                const Tc eA = Wt[mA], eB = Wt[mB];
+                const Tc dA = CD ? Dt[mA] : Dg[mA], dB = CD ? Dt[mB] : Dg[mB];
+                const double cEA = g.cE[iAc], cWA = g.cW[iAc], cEB = g.cE[iBc], cWB = g.cW[iBc];
+                const double pA = pr[iA], pB = pr[iA + 64];
+                const double dnA = defect_update(cEA, oEA, cWA, oWA, cN, oNA, cS, oSA, cF, oFA, cB, oBA, dA, eA);
+                const double dnB = defect_update(cEB, oEB, cWB, oWB, cN, oNB, cS, oSB, cF, oFB, cB, oBB, dB, eB);
+                if (tA < nown) {
+                    if (CD) Dt[mA] = (Tc)dnA;
+                    else Dg[mA] = (Tc)dnA;
+                    pr[iA] = pA + (double)eA;
+                }
+                if (tA + 32 < nown) {
+                    if (CD) Dt[mB] = (Tc)dnB;
+                    else Dg[mB] = (Tc)dnB;
+                    pr[iA + 64] = pB + (double)eB;
+                }
             }
         }
     };
@@ -575,7 +597,7 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
     // another cycle only when this one ended on its length
     if (failed || conv || nonfinite || done_c < cycle_len || ik0 + done >= itmax) break;
     // restart: the black ring again (the neighbours' final black rows; the red one is
-    // current), p += e, d = the FP64 defect of p + e, e = 0.  No grid barrier: the
+    // current), d = the FP64 defect of p + e and p += e in one pass, e = 0.  No grid barrier: the
     // next cycle's first red half reads a zero black ring, and its black half reads
     // red rows published after the next barrier.
     {
@@ -583,7 +605,6 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         fill_issue(0, fv);
         fill_commit(0, fv);
     }
-    add_e_to_p();
     update_defect();
     __syncthreads();
     zero_tile();
