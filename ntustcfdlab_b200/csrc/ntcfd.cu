@@ -104,6 +104,7 @@ struct ntcfd_ctx {
     double *faceW = nullptr, *faceE = nullptr, *faceS = nullptr, *faceN = nullptr;
     double *faceB = nullptr, *faceF = nullptr;
     double* outbuf = nullptr;   // pre, uc, vc, wc
+    double* stage = nullptr;    // one halo array, contiguous: host <-> device copies of the state
     double *coordY = nullptr, *coordZ = nullptr;  // node coordinates (pre-offset)
     double* coordbuf = nullptr;
     Ctl* ctl = nullptr;
@@ -1188,16 +1189,43 @@ static int set_mask_flag(ntcfd_ctx* ctx, bool nonzero) {
     return 0;
 }
 
+// A whole halo array (-1:n+2)^3 between its contiguous Fortran form s and the
+// padded natural layout d: one thread per element, i fastest; element a of an
+// axis is index a - 1.
+__global__ void k_halo_unpack(Geom g, const double* __restrict__ s, double* __restrict__ d) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    const int c = blockIdx.z * blockDim.z + threadIdx.z;
+    if (a >= g.nx + 4 || b >= g.ny + 4 || c >= g.nz + 4) return;
+    d[nat(g, a - 1, b - 1, c - 1)] = s[a + (size_t)(g.nx + 4) * (b + (size_t)(g.ny + 4) * c)];
+}
+__global__ void k_halo_pack(Geom g, const double* __restrict__ d, double* __restrict__ s) {
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y * blockDim.y + threadIdx.y;
+    const int c = blockIdx.z * blockDim.z + threadIdx.z;
+    if (a >= g.nx + 4 || b >= g.ny + 4 || c >= g.nz + 4) return;
+    s[a + (size_t)(g.nx + 4) * (b + (size_t)(g.ny + 4) * c)] = d[nat(g, a - 1, b - 1, c - 1)];
+}
+
+// A halo array between the host (the Fortran array, contiguous) and the
+// device field: one contiguous copy through the context's staging array and a
+// repacking kernel on the stream (a pitched 2-D copy moves the array as
+// (ny+4)(nz+4) rows of (nx+4) doubles and runs far below the link's
+// bandwidth).  The staging array is made on first use.
 static int copy_halo(ntcfd_ctx* ctx, double* dev, const double* host, bool to_dev) {
     const Geom& g = ctx->g;
-    double* d0 = dev + nat(g, -1, -1, -1);
-    const size_t w = (size_t)(g.nx + 4) * sizeof(double);
-    const size_t h = (size_t)(g.ny + 4) * (g.nz + 4);
-    if (to_dev)
-        CK(cudaMemcpy2DAsync(d0, g.px * sizeof(double), host, w, w, h, cudaMemcpyHostToDevice, ctx->stream));
-    else
-        CK(cudaMemcpy2DAsync((void*)host, w, d0, g.px * sizeof(double), w, h, cudaMemcpyDeviceToHost,
-                             ctx->stream));
+    const size_t n = (size_t)(g.nx + 4) * (g.ny + 4) * (g.nz + 4);
+    if (!ctx->stage)
+        if (int rc = dalloc(ctx, &ctx->stage, n)) return rc;
+    const dim3 b3(32, 4, 2), g3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2);
+    if (to_dev) {
+        CK(cudaMemcpyAsync(ctx->stage, host, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        k_halo_unpack<<<g3, b3, 0, ctx->stream>>>(g, ctx->stage, dev);
+    } else {
+        k_halo_pack<<<g3, b3, 0, ctx->stream>>>(g, dev, ctx->stage);
+        CK(cudaMemcpyAsync((void*)host, ctx->stage, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaGetLastError());
     return 0;
 }
 
