@@ -241,8 +241,9 @@ __global__ void k_make_rd(Geom g, SorCoef<Tc> sc, Tc* rdR, Tc* rdB) {
 // for KPT consecutive planes k; all loads of the KPT cells are issued before
 // any arithmetic so that a warp keeps 9*KPT loads in flight.  Offsets are
 // 32-bit (a grid holds fewer than 2^31 cells per colour array).  With
-// guard = 1 (several sweeps per loop body) the sweep is skipped once the
-// sweep budget (itmax, cycle length) is used up.  The block's max |change|
+// guard = 1 (several sweeps per loop body, or loop bodies queued ahead of the
+// host's decision) the sweep is skipped once the sweep budget (itmax, cycle
+// length) is used up or the solve has stopped.  The block's max |change|
 // goes to slot sub*kSpread + (block index mod kSpread).  It reads e as it is
 // (a cycle starts with k_clear_e); the first_mode argument of the row form is
 // not taken.
@@ -254,7 +255,7 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
                                               int guard, unsigned long long* slots, int /*first_mode*/) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
-        if (ik + sub >= itmax || inner + sub >= cycle_len) return;
+        if (ik + sub >= itmax || inner + sub >= cycle_len || ctl->converged || ctl->nonfinite) return;
     }
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -321,8 +322,9 @@ __global__ void __launch_bounds__(NT) k_sweep_cols(Geom g, SorCoef<Tc> sc, Tc* _
 // (a split row holds at least 2 + (nx+1)/2 entries, the tables nx + 5, and
 // the ghost rows and planes follow the interior ones), stores nothing and
 // leaves the change maximum alone.  With guard = 1 (several sweeps per loop
-// body) the sweep is skipped once the sweep budget (itmax, cycle length) is
-// used up.  The block's max |change| goes to slot
+// body, or loop bodies queued ahead of the host's decision) the sweep is
+// skipped once the sweep budget (itmax, cycle length) is used up or the solve
+// has stopped.  The block's max |change| goes to slot
 // sub*kSpread + (block index mod kSpread).  In a cycle's first sweep
 // (first_mode) e is zero everywhere before it, so the red half reads no e at
 // all and the black half none of its own.  rdOwn is not read: the diagonal
@@ -335,7 +337,7 @@ __global__ void __launch_bounds__(NT, 4) k_sweep_rows(Geom g, SorCoef<Tc> sc, Tc
                                               int guard, unsigned long long* slots, int first_mode) {
     if (guard) {
         const int ik = ctl->ik, inner = ctl->inner;
-        if (ik + sub >= itmax || inner + sub >= cycle_len) return;
+        if (ik + sub >= itmax || inner + sub >= cycle_len || ctl->converged || ctl->nonfinite) return;
     }
     const bool first = first_mode && ctl->inner + sub == 0;
     using B = decltype(abs_bits(Tc(0)));
@@ -477,6 +479,7 @@ __global__ void __launch_bounds__(NT, 3) k_defect_rows(Geom g, SorCoef<double> s
     const bool incr = ctl->cycles > 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         ctl->inner = 0;
+        ctl->pad_stop = 0;
         if (in_graph) cudaGraphSetConditional(inner, 1u);
     }
     const int lane = threadIdx.x & 31;
@@ -564,8 +567,11 @@ __global__ void __launch_bounds__(NT, 3) k_defect_rows(Geom g, SorCoef<double> s
 
 // One warp: the max over the kSpread slots of that sweep is its max|change|.
 // Outside a graph (in_graph = 0) the host reads ctl and takes the decision.
+// A test queued after the cycle's stop (bodies queued ahead of the host's
+// decision; their sweeps skip) leaves everything as it is.
 __global__ void k_sor_check(Ctl* ctl, unsigned long long* slots, int csweeps, int itmax,
                             int cycle_len, double zeta, cudaGraphConditionalHandle inner, int in_graph) {
+    if (ctl->pad_stop) return;
     const int lane = threadIdx.x;
     const int ik = ctl->ik, in = ctl->inner;
     int ran = csweeps;
@@ -624,6 +630,7 @@ __global__ void __launch_bounds__(256) k_correct_last(Geom g, double* p, const T
 __global__ void k_sor_begin(Ctl* ctl, int itmax, cudaGraphConditionalHandle outer, int in_graph) {
     ctl->ik = 0;
     ctl->inner = 0;
+    ctl->pad_stop = 0;
     ctl->cycles = 0;
     ctl->restarts = 0;
     ctl->bodies = 0;

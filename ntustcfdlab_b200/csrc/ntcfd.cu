@@ -42,6 +42,7 @@ constexpr int kSweepBy = 4;
 constexpr int kSweepKpt = 4;
 constexpr int kResNT = 512;      // threads per CTA of the resident SOR kernel
 constexpr int kMixedCycle = 8;   // default FP32 sweeps per defect-correction cycle (mixed_cycle = 0)
+constexpr int kAdjQueued = 16;   // loop bodies an adjoint solve queues per host round trip (streaming)
 const double kZeroZeta = 0.0;
 const int kOne = 1;
 
@@ -648,9 +649,14 @@ int build_dyn_graph(ntcfd_ctx* ctx) {
 // with a stop test every check_every sweeps), on pressure `p` (interior
 // updated, ghosts read) with right-hand side `b`, stop rule max|change| <=
 // zeta, sweep cap itmax and relaxation omega.  *hc receives the final
-// control block.
+// control block.  With chunk > 1 the streaming path queues up to `chunk` loop
+// bodies (and at most a cycle's) before the host reads the control block:
+// the bodies queued after the stop do nothing (their sweeps skip, their
+// tests return), so the solve is the same with one host round trip per chunk
+// instead of one per body.  chunk = 1 keeps the graph's launches one for one.
 template <class Tc>
-int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int itmax, double omega, Ctl* hc) {
+int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int itmax, double omega, Ctl* hc,
+                    int chunk = 1) {
     const Geom g = ctx->g;
     cudaStream_t st = ctx->stream;
     const dim3 b3(32, 4, 2), g3 = grid3(g, b3);
@@ -679,7 +685,9 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
     }
     k_sor_begin<<<1, 1, 0, st>>>(ctx->ctl, itmax, 0, 0);
     bool more = itmax > 0;
-    const int big_guard = ctx->csweeps > 1 ? 1 : 0;
+    const int big_guard = ctx->csweeps > 1 || chunk > 1 ? 1 : 0;
+    const int cycle_bodies = std::max(1, ctx->cycle_len / ctx->csweeps);
+    const int queued = std::max(1, std::min(chunk, cycle_bodies));
     while (more) {
         {
             k_defect_rows<Tc, kSweepNT><<<sweep_grid(g, kSweepNT, ctx->defect_resident), kSweepNT, 0, st>>>(
@@ -687,16 +695,18 @@ int sor_solve_eager(ntcfd_ctx* ctx, double* p, const double* b, double zeta, int
             if (!kRowSweep<Tc>) k_clear_e<Tc><<<g3, b3, 0, st>>>(g, eR, eB);
             const dim3 bs = Sweep<Tc>::block(), gs = Sweep<Tc>::grid(g, ctx->row_resident);
             for (;;) {
-                for (int sub = 0; sub < ctx->csweeps; ++sub) {
-                    Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
-                        g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
-                    Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
-                        g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
-                        ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
+                for (int q = 0; q < queued; ++q) {
+                    for (int sub = 0; sub < ctx->csweeps; ++sub) {
+                        Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
+                            g, sc, eR, eB, dR, (const Tc*)ctx->rdR, 0, omega, ctx->ctl, sub, itmax,
+                            ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
+                        Sweep<Tc>::fn<<<gs, bs, 0, st>>>(
+                            g, sc, eB, eR, dB, (const Tc*)ctx->rdB, 1, omega, ctx->ctl, sub, itmax,
+                            ctx->cycle_len, big_guard, ctx->slots, kRowSweep<Tc> ? 1 : 0);
+                    }
+                    k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
+                                                  zeta, 0, 0);
                 }
-                k_sor_check<<<1, 32, 0, st>>>(ctx->ctl, ctx->slots, ctx->csweeps, itmax, ctx->cycle_len,
-                                              zeta, 0, 0);
                 if (int rc = read_ctl()) return rc;
                 if (h.pad_stop) break;
             }
@@ -2172,7 +2182,8 @@ int adjoint_step(ntcfd_ctx* ctx, AdjBufs& A, const double* su, const double* sv,
         else CK(cudaMemcpyAsync(A.zprev, A.z, N * sizeof(double), cudaMemcpyDeviceToDevice, st));
         Ctl h{};
         CK(cudaEventRecord(A.e0, st));
-        if (int rc = sor_solve_eager<Tc>(ctx, A.z, A.badj, zeta_rel * bmax, itmax, omega, &h)) return rc;
+        if (int rc = sor_solve_eager<Tc>(ctx, A.z, A.badj, zeta_rel * bmax, itmax, omega, &h, kAdjQueued))
+            return rc;
         CK(cudaEventRecord(A.e1, st));
         CK(cudaEventSynchronize(A.e1));
         float sms = 0.0f;

@@ -379,3 +379,43 @@ def test_force_kernels_run_only_with_a_mask():
         assert all(i.cDrag == 0.0 and i.cLift == 0.0 for i in info2)
     finally:
         s.close()
+
+
+def test_state_and_mask_copies_round_trip():
+    """ntcfd_set_state/get_state and set_mask/get_mask move whole halo arrays,
+    ghosts included, through the device staging array bit for bit, on a grid
+    whose rows are not a multiple of the row padding."""
+    from ntustcfdlab_b200.solver import gridder_equal
+    n = (13, 7, 5)
+    s = _solver(make_params(*n, Re=100.0, dt=1e-3, precision=FP64), gridder_equal(*n, 1.0, 1.0, 1.0))
+    try:
+        state = _random_state(s.halo_shape, 11)
+        s.set_state(*state)
+        for a, b in zip(state, s.get_state()):
+            np.testing.assert_array_equal(a, b)
+        eta = np.asfortranarray(np.random.default_rng(12).random(s.halo_shape))
+        s.set_mask(eta)
+        np.testing.assert_array_equal(s.get_mask(), eta)
+        # the state is unchanged by the mask copies through the same staging array
+        for a, b in zip(state, s.get_state()):
+            np.testing.assert_array_equal(a, b)
+    finally:
+        s.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_streaming_solve_without_sweeps_leaves_p(prec):
+    """itmax = 0: the streaming solve runs no correction cycle, and its final
+    p += e (the last cycle's e) adds nothing: the interior of p stays as it
+    was set."""
+    from ntustcfdlab_b200 import cases
+    c = cases.cavity(20, 400.0, 1e-3, 1, precision=prec)
+    s = _solver(params_copy(c.params, sor_path=SOR_STREAMING, itmax=0), c.grid)
+    try:
+        st = _random_state(s.halo_shape, 5)
+        s.set_state(*st)
+        info, rc = s.step(1)
+        assert rc == abi.NTCFD_NOT_CONVERGED and info[0].sor_iters == 0
+        np.testing.assert_array_equal(interior(s.get_state()[3]), interior(st[3]))
+    finally:
+        s.close()
