@@ -193,7 +193,10 @@ int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az, const dou
  * 50x50 sub-cells within half a cell diagonal of the surface, real*4 arithmetic. */
 int ntcfd_build_mask_cylinder(ntcfd_ctx* ctx, double zc, double yc, double r);
 
-/* Velocity and pressure halo arrays in and out (exact FP64 checkpoints). */
+/* Velocity and pressure halo arrays in and out (exact FP64 checkpoints).
+ * These calls and ntcfd_set_mask/get_mask copy each array in one piece
+ * through a device staging array of one halo array, which the context makes
+ * on the first such call and keeps until ntcfd_destroy. */
 int ntcfd_set_state(ntcfd_ctx* ctx, const double* u, const double* v,
                     const double* w, const double* p);
 int ntcfd_get_state(ntcfd_ctx* ctx, double* u, double* v, double* w, double* p);
