@@ -338,54 +338,86 @@ k_sor_resident(Geom g, SorCoef<Tc> sc, Brick br, double* __restrict__ p, const d
         }
     };
 
+    struct DefIn {
+        Tc* D;          // d of the row: shared (CD) or global
+        double* pr;     // natural row of p, i = 0
+        int nown, mA, iA;
+        Tc oEA, oWA, oNA, oSA, oFA, oBA, oEB, oWB, oNB, oSB, oFB, oBB, eA, eB, dA, dB;
+        double cEA, cWA, cEB, cWB, cN, cS, cF, cB, pA, pB;
+    };
+    // every load of the cells t0 + lane and t0 + lane + 32 of task rc = 2 * row + colour
+    auto def_load = [&](int rc, int t0) {
+        DefIn x;
+        const int row = rc >> 1, c = rc & 1;
+        const int jl = row % nj + 1, kl = row / nj + 1;
+        const int j = j0 + jl - 1, k = k0 + kl - 1;
+        const int r = ((j + k) ^ c) & 1;
+        x.nown = r ? nown1 : nown0;
+        x.cN = g.cN[j]; x.cS = g.cS[j]; x.cF = g.cF[k]; x.cB = g.cB[k];
+        const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
+        const Tc* O = (c ? S0 : S1) + sr;         // the other colour's tile row
+        const Tc* Wt = (c ? S1 : S0) + sr;        // this colour's
+        x.D = CD ? (c ? D1 : D0) + dr : (c ? dBg : dRg) + spl(g, 0, j, k);
+        x.pr = p + nat(g, 0, j, k);
+        const int tA = t0 + lane;
+        const int mA = tA + 2 - r, mB = mA + 32;
+        x.mA = mA;
+        x.iA = 2 * tA + 2 - r;
+        const int iAc = min(x.iA, g.nx + 2), iBc = min(x.iA + 64, g.nx + 2);
+        x.oEA = O[mA + r]; x.oWA = O[mA - 1 + r]; x.oNA = O[mx + mA]; x.oSA = O[mA - mx];
+        x.oFA = O[plane + mA]; x.oBA = O[mA - plane];
+        x.oEB = O[mB + r]; x.oWB = O[mB - 1 + r]; x.oNB = O[mx + mB]; x.oSB = O[mB - mx];
+        x.oFB = O[plane + mB]; x.oBB = O[mB - plane];
+        x.eA = Wt[mA]; x.eB = Wt[mB];
+        x.dA = x.D[mA]; x.dB = x.D[mB];
+        x.cEA = g.cE[iAc]; x.cWA = g.cW[iAc]; x.cEB = g.cE[iBc]; x.cWB = g.cW[iBc];
+        x.pA = x.pr[x.iA]; x.pB = x.pr[x.iA + 64];
+        return x;
+    };
+    auto def_finish = [&](const DefIn& x, int t0) {
+        const double dnA = defect_update(x.cEA, x.oEA, x.cWA, x.oWA, x.cN, x.oNA, x.cS, x.oSA, x.cF, x.oFA, x.cB,
+                                         x.oBA, x.dA, x.eA);
+        const double dnB = defect_update(x.cEB, x.oEB, x.cWB, x.oWB, x.cN, x.oNB, x.cS, x.oSB, x.cF, x.oFB, x.cB,
+                                         x.oBB, x.dB, x.eB);
+        const int tA = t0 + lane;
+        if (tA < x.nown) {
+            x.D[x.mA] = (Tc)dnA;
+            x.pr[x.iA] = x.pA + (double)x.eA;
+        }
+        if (tA + 32 < x.nown) {
+            x.D[x.mA + 32] = (Tc)dnB;
+            x.pr[x.iA + 64] = x.pB + (double)x.eB;
+        }
+    };
     // Restart of a correction cycle: d of every cell of the brick becomes the FP64
     // defect of p + e (defect_update), from the tiles (both rings current), and the
     // cycle's e goes to p in the same pass (add_e_to_p takes only the last cycle's);
-    // one warp per row and colour, lane t takes the cells t and t + 32 of each
-    // 64-cell chunk (consecutive m: each shared-memory load of the warp reads one
-    // tile without bank conflicts), every load of both issued before the FP64
-    // arithmetic.  A lane past the row's last cell reads inside the shared
-    // allocation, the padded d and rd arrays and the natural p array (ghost rows
+    // a warp per row and colour ("task"), lane t takes the cells t and t + 32 of
+    // each 64-cell chunk (consecutive m: each shared-memory load of the warp reads
+    // one tile without bank conflicts).  FP32 rows of 33-64 cells per colour (the
+    // kResWide1 instance) go two tasks at a time, every load of both (p from L2
+    // among them) issued before the FP64 arithmetic of either.  A lane past the row's last cell reads inside the
+    // shared allocation, the padded d arrays and the natural p array (ghost rows
     // and planes follow the brick's) and stores nothing.
     auto update_defect = [&]() {
-        for (int rc = warp; rc < 2 * nrows; rc += NWARP) {
-            const int row = rc >> 1, c = rc & 1;
-            const int jl = row % nj + 1, kl = row / nj + 1;
-            const int j = j0 + jl - 1, k = k0 + kl - 1;
-            const int r = ((j + k) ^ c) & 1;
-            const int nown = r ? nown1 : nown0;
-            const double cN = g.cN[j], cS = g.cS[j], cF = g.cF[k], cB = g.cB[k];
-            const int sr = (kl * RS + jl) * mx, dr = ((kl - 1) * JB + (jl - 1)) * mx;
-            const long long g0 = spl(g, 0, j, k);
-            const Tc* O = (c ? S0 : S1) + sr;         // the other colour's tile row
-            const Tc* Wt = (c ? S1 : S0) + sr;        // this colour's
-            Tc* Dt = (c ? D1 : D0) + dr;
-            Tc* Dg = (c ? dBg : dRg) + g0;
-            double* pr = p + nat(g, 0, j, k);
-            for (int t0 = 0; t0 < nown; t0 += 64) {
-                const int tA = t0 + lane;
-                const int mA = tA + 2 - r, mB = mA + 32;
-                const int iA = 2 * tA + 2 - r;
-                const int iAc = min(iA, g.nx + 2), iBc = min(iA + 64, g.nx + 2);
-                const Tc oEA = O[mA + r], oWA = O[mA - 1 + r], oNA = O[mx + mA], oSA = O[mA - mx];
-                const Tc oFA = O[plane + mA], oBA = O[mA - plane];
-                const Tc oEB = O[mB + r], oWB = O[mB - 1 + r], oNB = O[mx + mB], oSB = O[mB - mx];
-                const Tc oFB = O[plane + mB], oBB = O[mB - plane];
-                const Tc eA = Wt[mA], eB = Wt[mB];
-                const Tc dA = CD ? Dt[mA] : Dg[mA], dB = CD ? Dt[mB] : Dg[mB];
-                const double cEA = g.cE[iAc], cWA = g.cW[iAc], cEB = g.cE[iBc], cWB = g.cW[iBc];
-                const double pA = pr[iA], pB = pr[iA + 64];
-                const double dnA = defect_update(cEA, oEA, cWA, oWA, cN, oNA, cS, oSA, cF, oFA, cB, oBA, dA, eA);
-                const double dnB = defect_update(cEB, oEB, cWB, oWB, cN, oNB, cS, oSB, cF, oFB, cB, oBB, dB, eB);
-                if (tA < nown) {
-                    if (CD) Dt[mA] = (Tc)dnA;
-                    else Dg[mA] = (Tc)dnA;
-                    pr[iA] = pA + (double)eA;
-                }
-                if (tA + 32 < nown) {
-                    if (CD) Dt[mB] = (Tc)dnB;
-                    else Dg[mB] = (Tc)dnB;
-                    pr[iA + 64] = pB + (double)eB;
+        // (FP64, whose restarts are rare, and the other row shapes keep one task at a
+        // time: the pair makes those instances spill)
+        if (sizeof(Tc) == 4 && MODE == kResWide1) {
+            for (int rc = warp; rc < 2 * nrows; rc += 2 * NWARP) {
+                const bool two = rc + NWARP < 2 * nrows;
+                const DefIn xa = def_load(rc, 0);
+                const DefIn xb = def_load(two ? rc + NWARP : rc, 0);
+                def_finish(xa, 0);
+                if (two) def_finish(xb, 0);
+            }
+        } else {
+            for (int rc = warp; rc < 2 * nrows; rc += NWARP) {
+                const int row = rc >> 1;
+                const int r = ((j0 + row % nj + k0 + row / nj) ^ (rc & 1)) & 1;
+                const int nown = r ? nown1 : nown0;
+                for (int t0 = 0; t0 < nown; t0 += 64) {
+                    const DefIn xa = def_load(rc, t0);
+                    def_finish(xa, t0);
                 }
             }
         }
