@@ -25,13 +25,29 @@ constexpr int kP32Ring = 5;                              // planes k-2..k+2
 constexpr int kP32NT = kP32BX * kP32BY;
 constexpr int kP32Loads = (3 * kP32Plane + kP32NT - 1) / kP32NT;   // per thread per plane
 
-// Planes per block: chunks of the k range, sized for about four blocks per
-// SM over the grid.
-inline int p32_chunk(int nx, int ny, int nz, int sms) {
-    const int cols = ((nx + kP32BX - 1) / kP32BX) * ((ny + kP32BY - 1) / kP32BY);
-    int chunks = (4 * sms + cols - 1) / cols;
-    chunks = chunks < 1 ? 1 : (chunks > nz ? nz : chunks);
-    return (nz + chunks - 1) / chunks;
+// Planes per block: the k range in chunks of kc planes, the count of chunks
+// chosen so that whole waves of blocks fill the SMs.  A block computes kc
+// planes and stages 4 more in its prologue (counted as 2); with `resident`
+// blocks at once on the device the launch takes ceil(blocks / resident)
+// waves, and kc minimises waves x (kc + 2).  (A grid of 2.16 waves, as a
+// fixed four blocks per SM gave at 128^3, spends a third wave on a sixth of
+// the blocks.)
+inline int p32_chunk(int nx, int ny, int nz, int resident) {
+    const long long cols = (long long)((nx + kP32BX - 1) / kP32BX) * ((ny + kP32BY - 1) / kP32BY);
+    const long long res = resident > 0 ? resident : 1;
+    int best_kc = nz;
+    long long best = -1;
+    for (int kc = 1; kc <= nz; ++kc) {
+        const long long chunks = (nz + kc - 1) / kc;
+        if (kc > 1 && (nz + kc - 2) / (kc - 1) == chunks) continue;   // same chunks, fewer planes
+        const long long waves = (cols * chunks + res - 1) / res;
+        const long long cost = waves * (kc + 2);
+        if (best < 0 || cost < best) {
+            best = cost;
+            best_kc = kc;
+        }
+    }
+    return best_kc;
 }
 
 __global__ void __launch_bounds__(kP32NT, 2) k_predictor32(Geom g, Tabs<float> tb, PredArgs a, int kc) {

@@ -123,6 +123,7 @@ struct ntcfd_ctx {
     int res_grid = 0;
     int sm_count = 0;
     int row_resident = 1;                   // resident blocks of k_sweep_rows (its grid cap)
+    int p32_resident = 1;                   // and of k_predictor32 (its waves)
     int defect_resident = 1;                // and of k_defect_rows
     size_t smem_optin = 0;
     cudaGraph_t graph = nullptr;
@@ -425,7 +426,7 @@ void launch_predictor(ntcfd_ctx* ctx, cudaStream_t st) {
     const PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
                       P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
     if (qc && P.precision == NTCFD_MIXED) {
-        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->sm_count);
+        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->p32_resident);
         k_predictor32<<<p32_grid(g, kc), dim3(kP32BX, kP32BY), p32_smem(kc), st>>>(g, ctx->tpf, pa, kc);
     } else if (qc) k_predictor<double><<<g3, b3, 0, st>>>(g, ctx->tpd, pa);
     else if (P.scheme == NTCFD_QUICK) k_predictor_scheme<kSchemeQuick><<<g3, b3, 0, st>>>(g, ctx->tpd, pa, P.Cs);
@@ -456,7 +457,7 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
     PredArgs pa{ctx->u, ctx->v, ctx->w, P.LES && qc ? ctx->nut : nullptr, ctx->us, ctx->vs, ctx->ws,
                 P.dt, 1. / P.Re, P.LES, ctx->fb, (long long)ctx->nat_elems};
     if (qc && P.precision == NTCFD_MIXED) {
-        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->sm_count);
+        const int kc = p32_chunk(g.nx, g.ny, g.nz, ctx->p32_resident);
         GK(add_kernel_ex(&n, G, dep, k_predictor32, p32_grid(g, kc), dim3(kP32BX, kP32BY), p32_smem(kc), false,
                          g, ctx->tpf, pa, kc));
     } else if (qc) GK(add_kernel(&n, G, dep, k_predictor<double>, g3, b3, g, ctx->tpd, pa));
@@ -1050,6 +1051,10 @@ int ntcfd_create(const ntcfd_params* prm, ntcfd_ctx** out) {
         }
         ctx->row_resident = std::max(1, a) * ctx->sm_count;
         ctx->defect_resident = std::max(1, b) * ctx->sm_count;
+        int c = 1;
+        if (P.precision == NTCFD_MIXED)
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, k_predictor32, kP32NT, p32_smem(P.nz)));
+        ctx->p32_resident = std::max(1, c) * ctx->sm_count;
     }
     if ((rc = dalloc(ctx, &ctx->coordbuf, (size_t)(P.ny + 5) + (P.nz + 5) + 8))) return rc;
     ctx->coordY = ctx->coordbuf + 1;                  // Y[j] valid for j = -1..ny+3
