@@ -58,7 +58,7 @@ def _device_used_gb():
 
 
 def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int = 0, M: int = 25,
-             log=print) -> dict:
+             log=print, adj_omega: float = 0.0) -> dict:
     """Both precisions over the case's steps from its initial state (after two
     untimed steps for the graph instantiation and a reset).  With adjoint_K, the
     mixed run saves its state K steps before the end and, after the run, the
@@ -115,8 +115,9 @@ def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int
             if saved is not None:
                 s.set_state(*saved)
                 r = s.adjoint(adjoint_K, M, w_drag=0.0, w_lift=1.0, inflow=("Back", 2, 1), force_grad=False,
-                              adj_itmax=3000)
-                out["adjoint"] = {"K": adjoint_K, "M": M, "objective": "mean cLift over the last K steps",
+                              adj_itmax=3000, adj_omega=adj_omega)
+                out["adjoint"] = {"K": adjoint_K, "M": M, "adj_omega": adj_omega or 1.9,
+                                  "objective": "mean cLift over the last K steps",
                                   "J": r["J"], "dJ_dtheta_inflow": r["dJ_dtheta"], "dJ_dU": r["dJ_dU"],
                                   "total_ms": r["total_ms"], "forward_ms": r["forward_ms"],
                                   "recompute_ms": r["recompute_ms"], "solve_ms": r["solve_ms"],
@@ -134,7 +135,7 @@ def run_case(name: str, cycle: int = 8, steps: int | None = None, adjoint_K: int
                     s.set_state(*saved)
                     s.build_mask_smooth(m["az"], m["ay"], m["aoa"], m["zc"], m["yc"], width)
                     rb = s.adjoint(adjoint_K, M, w_drag=0.0, w_lift=1.0, inflow=("Back", 2, 1), force_grad=False,
-                                   adj_itmax=3000)
+                                   adj_itmax=3000, adj_omega=adj_omega)
                     out["adjoint_body"] = {"K": adjoint_K, "M": M, "mask": f"smoothed, width {width:.5f}",
                                            "J": rb["J"], "dJ_daoa_body_per_rad": rb["dJ_daoa_body"],
                                            "dJ_dtheta_inflow": rb["dJ_dtheta"], "total_ms": rb["total_ms"],
@@ -211,6 +212,9 @@ def main():
     ap.add_argument("--steps", type=int, default=None, help="override the configured step count")
     ap.add_argument("--adjoint", type=int, default=0, help="C5: adjoint of mean cLift over the last K steps")
     ap.add_argument("--out", default=None)
+    ap.add_argument("--adj-omega", type=float, default=0.0,
+                    help="SOR relaxation of the C5 adjoint solves (0: the library's 1.9); the best factor "
+                         "grows with the grid: 1.9 on C4, about 1.97 on C5")
     ap.add_argument("--moving", type=int, default=0,
                     help="instead: per-step cost of a moving body on c3 over this many steps")
     ap.add_argument("--kernel-times", default=None, metavar="CASE",
@@ -241,7 +245,7 @@ def main():
     for name in args.cases.split(","):
         name = name.strip()
         r = run_case(name, args.cycle, args.steps, args.adjoint if name == "c5" else 0,
-                     log=lambda m: print(m, flush=True))
+                     log=lambda m: print(m, flush=True), adj_omega=args.adj_omega)
         print(json.dumps(r), flush=True)
         res.append(r)
         if args.out:
