@@ -175,16 +175,19 @@ int ntcfd_build_mask_smooth(ntcfd_ctx* ctx, const double* az, const double* ay, 
  * work on the device, so each step would stall, and a caller whose device
  * memory is already handed out to its own allocator may find cudaMalloc
  * failing mid-run.  This variant keeps that scratch in one fixed array that
- * the library reserves on every device that loads it (2.25 MiB, held
+ * the library reserves on every device that loads it (2.5 MiB, held
  * until the process exits) and calls no cudaMalloc, cudaFree or other
- * allocating routine; ETA goes to the context's existing storage.
+ * allocating routine; ETA goes to the context's existing storage.  The
+ * polygon is turned, its cut cells found and compacted and their sub-cell
+ * fractions summed on the device; the call waits for the stream once, to
+ * read the tie count.
  *
  * Limits: npts <= 16384 polygon points and ny*nz <= 262144 cells in the
  * (k,j) plane; larger inputs return NTCFD_EINVAL before any device work.
  * The first call on a device looks up the array's device address (once per
  * device); make that first call before any stream capture.  All calls on a
- * device share the array: the tie counter and the cut-cell flags are cleared
- * by each call, and two calls that overlap on the GPU (from two host threads
+ * device share the array: its control block, counters and cut-cell flags
+ * are cleared by each call, and two calls that overlap on the GPU (from two host threads
  * or two contexts on one device) race on it. */
 int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az, const double* ay,
                                      int npts, double aoa_deg, double zc, double yc,

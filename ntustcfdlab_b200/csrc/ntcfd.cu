@@ -1957,13 +1957,21 @@ int ntcfd_build_mask_polygon(ntcfd_ctx* ctx, const double* az_in, const double* 
 }  // extern "C"
 
 // Scratch of ntcfd_build_mask_polygon_noalloc: one fixed device array per
-// device that loads the library.  Layout: az[kNaPoly], ay[kNaPoly] (double),
-// points[kNaCells], list[kNaCells] (int), the tie counter (int).
+// device that loads the library.  Layout (every offset a multiple of 256 B):
+// the body polygon az[npts], ay[npts] (room for kNaPoly points each, double),
+// the moved polygon (the same), the cut-cell flags and the compacted cut-cell
+// list (kNaCells int each), then the bounds A, B, C, E, the listed-cell count
+// and the tie counter (int), the rotation's cosine and sine (double) and a
+// control block whose step index and halt flag the mask kernels read.
 namespace {
-constexpr size_t kNaPointsOff = 2 * sizeof(double) * (size_t)kNaPoly;
-constexpr size_t kNaListOff = kNaPointsOff + sizeof(int) * (size_t)kNaCells;
-constexpr size_t kNaTiesOff = kNaListOff + sizeof(int) * (size_t)kNaCells;
-constexpr size_t kNaBytes = kNaTiesOff + 256;   // 2.25 MiB + 256 B
+constexpr size_t kNaPolyOff = 2 * sizeof(double) * (size_t)kNaPoly;
+constexpr size_t kNaFlagsOff = 2 * kNaPolyOff;
+constexpr size_t kNaListOff = kNaFlagsOff + sizeof(int) * (size_t)kNaCells;
+constexpr size_t kNaMetaOff = kNaListOff + sizeof(int) * (size_t)kNaCells;
+constexpr size_t kNaTrigOff = kNaMetaOff + 64;
+constexpr size_t kNaCtlOff = kNaMetaOff + 256;
+constexpr size_t kNaBytes = kNaCtlOff + 256;   // 2.5 MiB + 512 B
+static_assert(sizeof(Ctl) <= 256, "control block outgrew its scratch slot");
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_mask_scratch[kNaBytes];
@@ -1991,6 +1999,11 @@ int noalloc_scratch(ntcfd_ctx* ctx, unsigned char** out) {
 }
 }  // namespace
 
+// The whole ray casting runs on the device, as a moving body's mask does
+// (k_dyn_*): the polygon is turned and its bounds found on the device, the
+// cut cells are compacted there with an atomic counter, and the host reads
+// back only the tie count at the end, so the call makes one stream
+// synchronisation and no host-side copy of coordinates or flags.
 extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az_in, const double* ay_in,
                                                 int npts, double aoa, double zc, double yc, int* ties_out) {
     DEV();
@@ -2008,65 +2021,40 @@ extern "C" int ntcfd_build_mask_polygon_noalloc(ntcfd_ctx* ctx, const double* az
     if (int rc = set_mask_flag(ctx, true)) return rc;
     unsigned char* base = nullptr;
     if (int rc = noalloc_scratch(ctx, &base)) return rc;
-    double* daz = reinterpret_cast<double*>(base);
-    double* day = daz + kNaPoly;
-    int* points = reinterpret_cast<int*>(base + kNaPointsOff);
-    int* list = reinterpret_cast<int*>(base + kNaListOff);
-    int* ties = reinterpret_cast<int*>(base + kNaTiesOff);
-    // polygon transform of airfoil.f90:597-611 (host)
-    std::vector<double> az(az_in, az_in + npts), ay(ay_in, ay_in + npts);
+    DynMask m{};
+    m.base = reinterpret_cast<const double*>(base);
+    m.poly = reinterpret_cast<double*>(base + kNaPolyOff);
+    m.flags = reinterpret_cast<int*>(base + kNaFlagsOff);
+    m.list = reinterpret_cast<int*>(base + kNaListOff);
+    m.meta = reinterpret_cast<int*>(base + kNaMetaOff);
+    m.trig = reinterpret_cast<const double*>(base + kNaTrigOff);
+    m.npts = npts;
+    m.zc = zc;
+    m.yc = yc;
+    m.eta1 = ctx->outbuf;
+    Ctl* ctl = reinterpret_cast<Ctl*>(base + kNaCtlOff);
+    // the rotation of airfoil.f90:597-611 (pi = 4 atan(1) there); the array keeps
+    // the previous call's contents, so the control block (step 0, no halt) is
+    // cleared here and the counters by k_dyn_rotate, the flags by k_dyn_main
     const double PI = 4.0 * std::atan(1.0);
-    for (int i = 0; i < npts; ++i) {
-        az[i] = az[i] - 0.25;
-        az[i] = std::cos((-aoa) * PI / 180) * az[i] - std::sin((-aoa) * PI / 180) * ay[i];
-        ay[i] = std::sin((-aoa) * PI / 180) * az[i] + std::cos((-aoa) * PI / 180) * ay[i];
-        az[i] = az[i] + zc;
-        ay[i] = ay[i] + yc;
-        az[i] = az[i] + 0.25;
-    }
-    std::vector<double> Y(g.ny + 5), Z(g.nz + 5);
-    CK(cudaMemcpyAsync(Y.data(), ctx->coordbuf, (g.ny + 5) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(Z.data(), ctx->coordbuf + (g.ny + 5) + 4, (g.nz + 5) * sizeof(double),
-                       cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    double miny = ay[0], maxy = ay[0], minz = az[0], maxz = az[0];
-    for (int i = 1; i < npts; ++i) {
-        miny = std::min(miny, ay[i]); maxy = std::max(maxy, ay[i]);
-        minz = std::min(minz, az[i]); maxz = std::max(maxz, az[i]);
-    }
-    int A = 0, B = 0, C = 0, E = 0;   // airfoil.f90:615-654
-    for (int j = 1; j <= g.ny; ++j) if (Y[j + 1] > miny) { A = j - 1; break; }
-    for (int j = 1; j <= g.ny; ++j) if (Y[j + 1] > maxy) { B = j; break; }
-    for (int k = 1; k <= g.nz; ++k) if (Z[k + 1] > minz) { C = k - 1; break; }
-    for (int k = 1; k <= g.nz; ++k) if (Z[k + 1] > maxz) { E = k; break; }
-    // the array keeps the previous call's contents: clear the flags and the counter
-    CK(cudaMemsetAsync(points, 0, sizeof(int) * cells, ctx->stream));
-    CK(cudaMemsetAsync(ties, 0, sizeof(int), ctx->stream));
-    CK(cudaMemcpyAsync(daz, az.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(day, ay.data(), sizeof(double) * npts, cudaMemcpyHostToDevice, ctx->stream));
-    double* eta1 = ctx->outbuf;
-    k_ray_main<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(
-        g.ny, g.nz, ctx->coordY, ctx->coordZ, daz, day, npts, eta1, ties);
-    k_ray_points<<<(npts + 127) / 128, 128, 0, ctx->stream>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, daz,
-                                                                day, npts, A, B, C, E, points);
-    std::vector<int> hp(cells);
-    CK(cudaMemcpyAsync(hp.data(), points, sizeof(int) * cells, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    std::vector<int> hl;
-    for (size_t q = 0; q < cells; ++q)
-        if (hp[q]) hl.push_back((int)q);
-    if (!hl.empty()) {
-        CK(cudaMemcpyAsync(list, hl.data(), sizeof(int) * hl.size(), cudaMemcpyHostToDevice, ctx->stream));
-        k_ray_sub<256><<<(unsigned)hl.size(), 256, 0, ctx->stream>>>(g.nz, ctx->coordY, ctx->coordZ, daz,
-                                                                    day, npts, list, eta1, ties);
-    }
-    const dim3 b3(32, 4, 2);
-    k_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), b3, 0, ctx->stream>>>(
-        g, eta1, ctx->eta);
-    int hties = 0;
-    CK(cudaMemcpyAsync(&hties, ties, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    const double trig[2] = {std::cos((-aoa) * PI / 180), std::sin((-aoa) * PI / 180)};
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(ctl, 0, sizeof(Ctl), st));
+    CK(cudaMemcpyAsync((double*)m.trig, trig, sizeof trig, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((double*)m.base, az_in, sizeof(double) * npts, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync((double*)m.base + npts, ay_in, sizeof(double) * npts, cudaMemcpyHostToDevice, st));
+    k_dyn_rotate<512><<<1, 512, 0, st>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, m, ctl);
+    k_dyn_main<<<dim3((g.nz + 31) / 32, (g.ny + 7) / 8), dim3(32, 8), 0, st>>>(g.ny, g.nz, ctx->coordY,
+                                                                              ctx->coordZ, m, ctl);
+    k_dyn_points<<<(npts + 127) / 128, 128, 0, st>>>(g.ny, g.nz, ctx->coordY, ctx->coordZ, m, ctl);
+    k_dyn_compact<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>((int)cells, m, ctl);
+    k_dyn_sub<256><<<2 * ctx->sm_count, 256, 0, st>>>(g.nz, ctx->coordY, ctx->coordZ, m, ctl);
+    k_dyn_extrude<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 3) / 4, (g.nz + 4 + 1) / 2), dim3(32, 4, 2), 0, st>>>(
+        g, m.eta1, ctx->eta, ctl);
     CK(cudaGetLastError());
-    CK(cudaStreamSynchronize(ctx->stream));
+    int hties = 0;
+    CK(cudaMemcpyAsync(&hties, &m.meta[5], sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
     if (ties_out) *ties_out = hties;
     if (hties)
         return fail(ctx, NTCFD_EINVAL,

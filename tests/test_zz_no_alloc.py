@@ -53,6 +53,29 @@ def test_noalloc_mask_matches_allocating_entry_point():
     s.close()
 
 
+def test_noalloc_after_a_larger_call_on_another_context():
+    """The shared array still holds a larger plane's flags and list from the
+    call before; a smaller context's call must not see them."""
+    from ntustcfdlab_b200.solver import Solver, gridder_equal
+    s, z, y = _solver_and_polygon()
+    assert _noalloc(s, z, y, 7.0) == (0, 0), s._err()
+    n = (3, 40, 56)
+    s2 = Solver(make_params(*n, Re=100.0, dt=1e-3), gridder_equal(*n, 1.0, 2.0, 2.8))
+    try:
+        zs, ys = np.ascontiguousarray(z * 0.9), np.ascontiguousarray(y * 0.9)
+        assert s2.build_mask_polygon(zs, ys, 9.0, 1.1, 1.0) == 0
+        ref = s2.get_mask()
+        assert ref.sum() > 0
+        s2.set_mask(np.zeros(s2.halo_shape, order="F"))
+        for _ in range(2):
+            rc, ties = _noalloc(s2, zs, ys, 9.0, 1.1, 1.0)
+            assert rc == 0 and ties == 0, s2._err()
+            np.testing.assert_array_equal(s2.get_mask(), ref)
+    finally:
+        s2.close()
+        s.close()
+
+
 def test_noalloc_rejects_inputs_beyond_its_limits():
     s, z, y = _solver_and_polygon()
     big = np.ascontiguousarray(np.resize(z, 16385))
