@@ -173,17 +173,17 @@ __device__ __forceinline__ double tangential(int kind, double val, double inner,
     }
 }
 
-__device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, int k) {
+__device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, int k, int fld) {
     const int nx = g.nx;
     auto I = [&](int i) { return nat(g, i, j, k); };
     const bool inside = j >= 1 && j <= g.ny && k >= 1 && k <= g.nz;
-    if (inside) {
+    if (fld == 0 && inside) {
         const long long f = (long long)(k - 1) * g.ny + (j - 1);
         a.faceW[f] = a.u[I(0)];
         a.faceE[f] = a.u[I(nx)];
     }
     // West (boundary_conditions.f90:13-57)
-    {
+    if (fld == 0) {
         const int ku = a.bc[0][0];
         double u0;
         if (ku == BC_NOSLIP) u0 = 0.0;
@@ -192,8 +192,10 @@ __device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, i
         else u0 = a.u[I(nx)];
         a.u[I(0)] = u0;
         a.u[I(-1)] = (ku == BC_PERIODIC) ? a.u[I(nx - 1)] : u0;
+    } else if (fld <= 2) {
         double* f2[2] = {a.v, a.w};
-        for (int c = 1; c <= 2; ++c) {
+        {
+            const int c = fld;
             double* f = f2[c - 1];
             const int kd = a.bc[0][c];
             const double g0 = tangential(kd, a.val[0][c], f[I(1)], f[I(nx)]);
@@ -202,7 +204,7 @@ __device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, i
         }
     }
     // East (boundary_conditions.f90:59-105)
-    {
+    if (fld == 0) {
         const int ku = a.bc[1][0];
         if (ku == BC_PERIODIC) {
             a.u[I(nx + 1)] = a.u[I(1)];
@@ -216,8 +218,10 @@ __device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, i
             a.u[I(nx + 1)] = un;
             a.u[I(nx + 2)] = un;
         }
+    } else if (fld <= 2) {
         double* f2[2] = {a.v, a.w};
-        for (int c = 1; c <= 2; ++c) {
+        {
+            const int c = fld;
             double* f = f2[c - 1];
             const int kd = a.bc[1][c];
             if (kd == BC_PERIODIC) {
@@ -231,6 +235,7 @@ __device__ __forceinline__ void bc_x_at(const Geom& g, const BcArgs& a, int j, i
         }
     }
     // pressure (boundary_conditions.f90:329-342)
+    if (fld != 3) return;
     if (a.bc[0][0] == BC_PERIODIC) {
         a.p[I(0)] = a.p[I(nx)]; a.p[I(-1)] = a.p[I(nx - 1)];
         a.p[I(nx + 1)] = a.p[I(1)]; a.p[I(nx + 2)] = a.p[I(2)];
@@ -245,25 +250,25 @@ __global__ void k_bc_x(Geom g, BcArgs a) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x - 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
     if (j > g.ny + 2 || k > g.nz + 2) return;
-    bc_x_at(g, a, j, k);
+    bc_x_at(g, a, j, k, blockIdx.z);
 }
 
-__device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, int k) {
+__device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, int k, int fld) {
     const int ny = g.ny;
     auto J = [&](int j) { return nat(g, i, j, k); };
-    if (i >= 1 && i <= g.nx && k >= 1 && k <= g.nz) {
+    if (fld == 1 && i >= 1 && i <= g.nx && k >= 1 && k <= g.nz) {
         const long long f = (long long)(k - 1) * g.nx + (i - 1);
         a.faceS[f] = a.v[J(0)];
         a.faceN[f] = a.v[J(ny)];
     }
     // South (boundary_conditions.f90:107-153): u, v, w
-    {
+    if (fld == 0) {
         const int kd = a.bc[2][0];
         const double g0 = tangential(kd, a.val[2][0], a.u[J(1)], a.u[J(ny)]);
         a.u[J(0)] = g0;
         a.u[J(-1)] = (kd == BC_PERIODIC) ? a.u[J(ny - 1)] : g0;
     }
-    {
+    if (fld == 1) {
         const int kv = a.bc[2][1];
         double v0;
         if (kv == BC_NOSLIP) v0 = 0.0;
@@ -273,14 +278,14 @@ __device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, i
         a.v[J(0)] = v0;
         a.v[J(-1)] = (kv == BC_PERIODIC) ? a.v[J(ny - 1)] : v0;
     }
-    {
+    if (fld == 2) {
         const int kd = a.bc[2][2];
         const double g0 = tangential(kd, a.val[2][2], a.w[J(1)], a.w[J(ny)]);
         a.w[J(0)] = g0;
         a.w[J(-1)] = (kd == BC_PERIODIC) ? a.w[J(ny - 1)] : g0;
     }
     // North (boundary_conditions.f90:155-202)
-    {
+    if (fld == 0) {
         const int kd = a.bc[3][0];
         if (kd == BC_PERIODIC) { a.u[J(ny + 1)] = a.u[J(1)]; a.u[J(ny + 2)] = a.u[J(2)]; }
         else {
@@ -288,7 +293,7 @@ __device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, i
             a.u[J(ny + 1)] = g1; a.u[J(ny + 2)] = g1;
         }
     }
-    {
+    if (fld == 1) {
         const int kv = a.bc[3][1];
         if (kv == BC_PERIODIC) { a.v[J(ny + 1)] = a.v[J(1)]; a.v[J(ny + 2)] = a.v[J(2)]; }
         else {
@@ -299,7 +304,7 @@ __device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, i
             a.v[J(ny)] = vn; a.v[J(ny + 1)] = vn; a.v[J(ny + 2)] = vn;
         }
     }
-    {
+    if (fld == 2) {
         const int kd = a.bc[3][2];
         if (kd == BC_PERIODIC) { a.w[J(ny + 1)] = a.w[J(1)]; a.w[J(ny + 2)] = a.w[J(2)]; }
         else {
@@ -308,6 +313,7 @@ __device__ __forceinline__ void bc_y_at(const Geom& g, const BcArgs& a, int i, i
         }
     }
     // pressure (boundary_conditions.f90:344-358)
+    if (fld != 3) return;
     if (a.bc[2][1] == BC_PERIODIC) {
         a.p[J(0)] = a.p[J(ny)]; a.p[J(-1)] = a.p[J(ny - 1)];
         a.p[J(ny + 1)] = a.p[J(1)]; a.p[J(ny + 2)] = a.p[J(2)];
@@ -322,33 +328,34 @@ __global__ void k_bc_y(Geom g, BcArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
     const int k = blockIdx.y * blockDim.y + threadIdx.y - 1;
     if (i > g.nx + 2 || k > g.nz + 2) return;
-    bc_y_at(g, a, i, k);
+    bc_y_at(g, a, i, k, blockIdx.z);
 }
 
-__device__ __forceinline__ void bc_z_at(const Geom& g, const BcArgs& a, int i, int j) {
+__device__ __forceinline__ void bc_z_at(const Geom& g, const BcArgs& a, int i, int j, int fld) {
     const int nz = g.nz;
     auto K = [&](int k) { return nat(g, i, j, k); };
-    if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
+    if (fld == 2 && i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
         const long long f = (long long)(j - 1) * g.nx + (i - 1);
         a.faceB[f] = a.w[K(0)];
         a.faceF[f] = a.w[K(nz)];
     }
     // Back (boundary_conditions.f90:205-252): u, v tangential, w normal.  A face
     // shared with the neighbouring z-slab keeps the planes the exchange wrote.
-    if (a.bc[4][0] != BC_INTERFACE) {
+    if (a.bc[4][0] != BC_INTERFACE && fld <= 1) {
         double* f2[2] = {a.u, a.v};
-        for (int c = 0; c < 2; ++c) {
-            double* f = f2[c];
-            const int kd = a.bc[4][c];
-            if (kd == BC_NEUMANN && c == 1) {
-                // BackWall_v 'Neumann' assigns v(i,j,0) to itself (boundary_conditions.f90:228)
-                f[K(-1)] = f[K(0)];
-                continue;
-            }
+        const int c = fld;
+        double* f = f2[c];
+        const int kd = a.bc[4][c];
+        if (kd == BC_NEUMANN && c == 1) {
+            // BackWall_v 'Neumann' assigns v(i,j,0) to itself (boundary_conditions.f90:228)
+            f[K(-1)] = f[K(0)];
+        } else {
             const double g0 = tangential(kd, a.val[4][c], f[K(1)], f[K(nz)]);
             f[K(0)] = g0;
             f[K(-1)] = (kd == BC_PERIODIC) ? f[K(nz - 1)] : g0;
         }
+    }
+    if (a.bc[4][0] != BC_INTERFACE && fld == 2) {
         const int kw = a.bc[4][2];
         double w0;
         if (kw == BC_NOSLIP) w0 = 0.0;
@@ -359,17 +366,18 @@ __device__ __forceinline__ void bc_z_at(const Geom& g, const BcArgs& a, int i, i
         a.w[K(-1)] = (kw == BC_PERIODIC) ? a.w[K(nz - 1)] : w0;
     }
     // Front (boundary_conditions.f90:255-301)
-    if (a.bc[5][0] != BC_INTERFACE) {
+    if (a.bc[5][0] != BC_INTERFACE && fld <= 1) {
         double* f2[2] = {a.u, a.v};
-        for (int c = 0; c < 2; ++c) {
-            double* f = f2[c];
-            const int kd = a.bc[5][c];
-            if (kd == BC_PERIODIC) { f[K(nz + 1)] = f[K(1)]; f[K(nz + 2)] = f[K(2)]; }
-            else {
-                const double g1 = tangential(kd, a.val[5][c], f[K(nz)], 0.0);
-                f[K(nz + 1)] = g1; f[K(nz + 2)] = g1;
-            }
+        const int c = fld;
+        double* f = f2[c];
+        const int kd = a.bc[5][c];
+        if (kd == BC_PERIODIC) { f[K(nz + 1)] = f[K(1)]; f[K(nz + 2)] = f[K(2)]; }
+        else {
+            const double g1 = tangential(kd, a.val[5][c], f[K(nz)], 0.0);
+            f[K(nz + 1)] = g1; f[K(nz + 2)] = g1;
         }
+    }
+    if (a.bc[5][0] != BC_INTERFACE && fld == 2) {
         const int kw = a.bc[5][2];
         if (kw == BC_PERIODIC) { a.w[K(nz + 1)] = a.w[K(1)]; a.w[K(nz + 2)] = a.w[K(2)]; }
         else {
@@ -381,6 +389,7 @@ __device__ __forceinline__ void bc_z_at(const Geom& g, const BcArgs& a, int i, i
         }
     }
     // pressure (boundary_conditions.f90:360-374)
+    if (fld != 3) return;
     if (a.bc[4][2] == BC_PERIODIC) {
         a.p[K(0)] = a.p[K(nz)]; a.p[K(-1)] = a.p[K(nz - 1)];
         a.p[K(nz + 1)] = a.p[K(1)]; a.p[K(nz + 2)] = a.p[K(2)];
@@ -395,8 +404,16 @@ __global__ void k_bc_z(Geom g, BcArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x - 1;
     const int j = blockIdx.y * blockDim.y + threadIdx.y - 1;
     if (i > g.nx + 2 || j > g.ny + 2) return;
-    bc_z_at(g, a, i, j);
+    bc_z_at(g, a, i, j, blockIdx.z);
 }
+
+// Launch grids of k_bc_x/y/z: 32 x 8 threads over the face's (ghost-inclusive)
+// rows, one z layer per field (u, v, w, p).  The fields of a face are
+// independent, so the four layers run side by side: each thread keeps one
+// field's short load/store chain instead of all four in sequence.
+inline dim3 bc_grid_x(const Geom& g) { return dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8, 4); }
+inline dim3 bc_grid_y(const Geom& g) { return dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8, 4); }
+inline dim3 bc_grid_z(const Geom& g) { return dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8, 4); }
 
 // ---------------------------------------------------------------- K8 ----
 // Centred output (calcul_new_velocity.f90:171-181) and pre = p (GS.f90:86-94),

@@ -564,11 +564,11 @@ int add_step_nodes(ntcfd_ctx* ctx, cudaGraph_t G, int extra) {
     std::memcpy(ba.val, P.bc_value, sizeof ba.val);
     ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
     ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
-    GK(add_kernel(&n, G, dep, k_bc_x, dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), g, ba));
+    GK(add_kernel(&n, G, dep, k_bc_x, bc_grid_x(g), dim3(32, 8), g, ba));
     dep = {n};
-    GK(add_kernel(&n, G, dep, k_bc_y, dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), g, ba));
+    GK(add_kernel(&n, G, dep, k_bc_y, bc_grid_y(g), dim3(32, 8), g, ba));
     dep = {n};
-    GK(add_kernel(&n, G, dep, k_bc_z, dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), g, ba));
+    GK(add_kernel(&n, G, dep, k_bc_z, bc_grid_z(g), dim3(32, 8), g, ba));
     dep = {n};
     if (P.diag_divergence) {
         GK(add_kernel(&n, G, dep, k_divmax<256>, g3, b3, g, (const double*)ctx->u,
@@ -749,9 +749,9 @@ int run_step_eager(ntcfd_ctx* ctx) {
     std::memcpy(ba.val, P.bc_value, sizeof ba.val);
     ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
     ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
-    k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
-    k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
-    k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+    k_bc_x<<<bc_grid_x(g), dim3(32, 8), 0, st>>>(g, ba);
+    k_bc_y<<<bc_grid_y(g), dim3(32, 8), 0, st>>>(g, ba);
+    k_bc_z<<<bc_grid_z(g), dim3(32, 8), 0, st>>>(g, ba);
     if (P.diag_divergence) k_divmax<256><<<g3, b3, 0, st>>>(g, ctx->u, ctx->v, ctx->w, ctx->divslot);
     const int fixed = 7 + (ctx->mask_nonzero ? 2 : 0) + (P.LES ? 1 : 0) + (P.diag_divergence ? 1 : 0) +
                       (ctx->resident ? 0 : 2);
@@ -929,9 +929,9 @@ int time_kernels_t(ntcfd_ctx* ctx, int reps, ntcfd_kernel_times* out) {
     ba.faceW = junk; ba.faceE = junk + (size_t)g.ny * g.nz; ba.faceS = ba.faceE + (size_t)g.ny * g.nz;
     ba.faceN = ba.faceS + nxz; ba.faceB = ba.faceN + nxz; ba.faceF = ba.faceB + nxy;
     if ((rc = timed([&] {
-             k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
-             k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
-             k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+             k_bc_x<<<bc_grid_x(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+             k_bc_y<<<bc_grid_y(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+             k_bc_z<<<bc_grid_z(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
          }, &out->bc_ms, 1)))
         return rc;
     return 0;
@@ -1298,9 +1298,9 @@ int ntcfd_apply_bc(ntcfd_ctx* ctx) {
     std::memcpy(ba.val, ctx->prm.bc_value, sizeof ba.val);
     ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
     ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
-    k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
-    k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
-    k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    k_bc_x<<<bc_grid_x(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    k_bc_y<<<bc_grid_y(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
+    k_bc_z<<<bc_grid_z(g), dim3(32, 8), 0, ctx->stream>>>(g, ba);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(ctx->stream));
     return 0;
@@ -1679,9 +1679,9 @@ int ntcfd_slab_stage(ntcfd_ctx* ctx, int stage, int colour) {
             std::memcpy(ba.val, P.bc_value, sizeof ba.val);
             ba.faceW = ctx->faceW; ba.faceE = ctx->faceE; ba.faceS = ctx->faceS;
             ba.faceN = ctx->faceN; ba.faceB = ctx->faceB; ba.faceF = ctx->faceF;
-            k_bc_x<<<dim3((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
-            k_bc_y<<<dim3((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
-            k_bc_z<<<dim3((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), dim3(32, 8), 0, st>>>(g, ba);
+            k_bc_x<<<bc_grid_x(g), dim3(32, 8), 0, st>>>(g, ba);
+            k_bc_y<<<bc_grid_y(g), dim3(32, 8), 0, st>>>(g, ba);
+            k_bc_z<<<bc_grid_z(g), dim3(32, 8), 0, st>>>(g, ba);
             ctx->time = ctx->time + P.dt;
             ctx->istep += 1;
             break;
@@ -2302,9 +2302,9 @@ int adjoint_t(ntcfd_ctx* ctx, const ntcfd_adj_spec* sp, ntcfd_adj_result* res, d
     const dim3 gbx((g.ny + 4 + 31) / 32, (g.nz + 4 + 7) / 8), gby((g.nx + 4 + 31) / 32, (g.nz + 4 + 7) / 8),
         gbz((g.nx + 4 + 31) / 32, (g.ny + 4 + 7) / 8), bbc(32, 8);
     if (sp->initial_bc) {
-        k_bc_x<<<gbx, bbc, 0, st>>>(g, ba);
-        k_bc_y<<<gby, bbc, 0, st>>>(g, ba);
-        k_bc_z<<<gbz, bbc, 0, st>>>(g, ba);
+        k_bc_x<<<bc_grid_x(g), bbc, 0, st>>>(g, ba);
+        k_bc_y<<<bc_grid_y(g), bbc, 0, st>>>(g, ba);
+        k_bc_z<<<bc_grid_z(g), bbc, 0, st>>>(g, ba);
         CK(cudaGetLastError());
     }
     // ---- forward pass: K steps, a checkpoint every M, the guards of every step
